@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the plain complex128 state-vector path at 30 qubits.
+
+Workload (one step): a 30-qubit complex128 register (16 GiB) starts in
+|0..0>; a seeded depth-40 random circuit is applied (per layer U3 on all 30
+qubits with angles ~ U[0, 2pi), then a CZ/CNOT brickwork; 5 % of the gates get
+1-3 extra random controls / anticontrols; 1780 gates); then all 30 single-qubit
+probabilities, measurement with collapse of 4 random qubits (30 -> 26 qubits)
+and the reduced density matrix of qubits 0-9 (1024 x 1024, copied to the host).
+
+metric: gate-layers per second (40 per step), whole job over all GPUs.
+  value -- device time (CUDA events on the engine's stream) from the first
+           queued sweep to the last result, gates already queued;
+  e2e   -- host wall time of the same job through the public `doki` API,
+           gate matrices created from host memory and every result read back.
+--gpus N runs N independent replicas (the path does not shard at this size).
+--impl reference times the reference Doki CPU module (compiled from source
+into oracle/_ref) on the host cores, one workload gate per step.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "30q gate-layers/s"
+UNIT = "gate-layers/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--qubits", type=int, default=30)
+    p.add_argument("--depth", type=int, default=40)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fusion", action="store_true",
+                   help="one sweep per gate (the per-gate plain method)")
+    return p.parse_args()
+
+
+def workload_config(n, depth, c):
+    return {
+        "workload": (f"{n}-qubit complex128 register, seeded depth-{depth} random circuit "
+                     "(U3 on all qubits + CZ/CNOT brickwork, 5% gates with 1-3 extra "
+                     "controls/anticontrols), all marginals, measure+collapse of 4 qubits, "
+                     "reduced density matrix of qubits 0-9"),
+        "qubits": n, "depth": depth, "gates": len(c.ops),
+        "state_bytes": 16 << n,
+        "l2": "inputs larger than L2 (state 16 GiB vs 126 MB L2)",
+        "parallelism": "replicas",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "sweep_c128_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------------ engine --
+
+def run_job(d, c, gates, keep, rolls_mask, rolls):
+    """One full workload through the public API; returns the host results."""
+    n = c.num_qubits
+    reg = d.registry_new(n, False)
+    for op, g in zip(c.ops, gates):
+        ctl = set(op.controls) if (op.controls or op.anticontrols) else None
+        reg = d.registry_apply(reg, g, list(op.targets), ctl, set(op.anticontrols) or None,
+                               -1, False)
+    return reg
+
+
+def finish_job(d, reg, n, keep, mask, rolls):
+    probs = [d.registry_prob(reg, q, -1, False) for q in range(n)]
+    sub, res = d.registry_measure(reg, mask, rolls, -1, False)
+    rho = d.registry_density(reg, False)
+    for e in range(n - 1, keep - 1, -1):
+        rho = d.funmatrix_partialtrace(rho, e, False)
+    mat = d.funmatrix_numpy(rho)
+    return probs, res, mat
+
+
+def engine_arm(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    if world > 1:
+        os.environ["DK_DEVICE"] = str(local_rank)
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        torch.distributed.init_process_group(
+            "nccl", timeout=datetime.timedelta(seconds=300),
+            device_id=torch.device("cuda", local_rank))
+
+    import doki_b200
+    from doki_b200 import workloads as W
+
+    d = doki_b200.load()
+    if args.no_fusion:
+        d.engine_set_fusion(False)
+    n, depth, keep = args.qubits, args.depth, min(10, args.qubits)
+    c = W.scale_circuit(seed=2, n=n, depth=depth, keep=keep)
+    mask, rolls = c.measure_mask, c.rolls.tolist()
+    gates = [d.gate_new(op.k, op.gate.tolist(), False) for op in c.ops]
+
+    # warm-up (also creates the engine stream)
+    for _ in range(args.warmup):
+        reg = run_job(d, c, gates, keep, mask, rolls)
+        finish_job(d, reg, n, keep, mask, rolls)
+        del reg
+    d.engine_sync()
+    stream = torch.cuda.ExternalStream(d.engine_stream(), device=torch.device("cuda", local_rank))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # ---- device-timed value --------------------------------------------
+    clocks = ClockSampler(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    st0 = d.engine_stats()
+    dev_ms, sweep_ms, nsweeps = 0.0, 0.0, 0
+    for _ in range(args.steps):
+        reg = run_job(d, c, gates, keep, mask, rolls)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        s_before = d.engine_stats()["sweeps"]
+        d.registry_flush(reg)
+        e1.record(stream)
+        nsweeps += d.engine_stats()["sweeps"] - s_before
+        finish_job(d, reg, n, keep, mask, rolls)
+        e2.record(stream)
+        e2.synchronize()
+        dev_ms += e0.elapsed_time(e2)
+        sweep_ms += e0.elapsed_time(e1)
+        del reg
+    d.engine_sync()
+    torch.cuda.synchronize()
+    st1 = d.engine_stats()
+    clk = clocks.stop()
+    barrier()
+
+    # ---- end-to-end through the public API -------------------------------
+    e2e_s = 0.0
+    io0 = d.engine_stats()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        g2 = [d.gate_new(op.k, op.gate.tolist(), False) for op in c.ops]
+        reg = run_job(d, c, g2, keep, mask, rolls)
+        probs, res, mat = finish_job(d, reg, n, keep, mask, rolls)
+        e2e_s += time.perf_counter() - t0
+        del reg, g2
+    io1 = d.engine_stats()
+    barrier()
+
+    if world > 1:
+        t = torch.tensor([dev_ms, e2e_s, sweep_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        dev_ms, e2e_s, sweep_ms = t.tolist()
+
+    layers = depth * args.steps
+    value = world * layers / (dev_ms / 1e3)
+    e2e_value = world * layers / e2e_s
+    state_bytes = 16 << n
+    avg_sweep_s = (sweep_ms / 1e3) / max(1, nsweeps)
+    achieved = 2 * state_bytes / avg_sweep_s / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    tr = committed_traffic()
+    traffic = None
+    if tr and tr.get("qubits"):
+        traffic = float(tr["bytes_per_launch"]) * (state_bytes / (16 << int(tr["qubits"])))
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(n, depth, c),
+        "roofline": {"bound": "hbm", "kernel": "k_sweep<double> (fused gate sweep)",
+                     "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind + " hbm_gbs (copy)", "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": 2 * state_bytes,
+                     "avg_launch_ms": avg_sweep_s * 1e3,
+                     "sweeps_per_step": nsweeps / args.steps,
+                     "gates_per_step": len(c.ops)},
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": (io1["h2d_bytes"] - io0["h2d_bytes"]) // args.steps,
+                "d2h_bytes_per_step": (io1["d2h_bytes"] - io0["d2h_bytes"]) // args.steps},
+        "gpu_launches": st1["kernel_launches"] - st0["kernel_launches"],
+        "clocks": clk,
+        "fusion": not args.no_fusion,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(n, c)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# --------------------------------------------------------------- reference --
+
+def sample_ops(c):
+    """Gates of the first layer, spread over low / high qubits and 2-qubit ops."""
+    layer = c.ops[c.layer_starts[0]:c.layer_starts[1]]
+    idx = [0, len(layer) // 2 - 1, len(layer) - 1, 7, len(layer) // 2 + 3, 15]
+    return [layer[i % len(layer)] for i in idx]
+
+
+def reference_timings(n, c, count, warm=0):
+    from oracle import oracle as O
+    from doki_b200 import workloads as W
+    ref = O.reference_module()
+    threads = os.cpu_count() or 1
+    ops = sample_ops(c)
+    reg = ref.registry_new(n, False)
+    times = []
+    for i in range(warm + count):
+        op = ops[i % len(ops)]
+        g = ref.gate_new(op.k, op.gate.tolist(), False)
+        ctl = set(op.controls) if (op.controls or op.anticontrols) else None
+        t0 = time.perf_counter()
+        new = ref.registry_apply(reg, g, list(op.targets), ctl,
+                                 set(op.anticontrols) or None, threads, False)
+        dt = time.perf_counter() - t0
+        del reg
+        reg = new
+        if i >= warm:
+            times.append(dt)
+    del reg
+    return times, threads
+
+
+def cpu_baseline(n, c):
+    gates_per_layer = len(c.ops) / c.depth
+    try:
+        times, threads = reference_timings(n, c, 4)
+        qn = n
+    except MemoryError:
+        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                "sample": "host memory too small for the reference at this size"}
+    per_gate = statistics.mean(times)
+    return {"value": 1.0 / (per_gate * gates_per_layer), "unit": UNIT, "cores": threads,
+            "kind": "reference",
+            "sample": (f"reference doki registry_apply (OpenMP, {threads} threads) on {qn} "
+                       f"qubits: {len(times)} gates from layer 0 (low/high U3, CNOT/CZ), "
+                       f"mean {per_gate:.3f} s/gate x {gates_per_layer:.1f} gates/layer")}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from doki_b200 import workloads as W
+    from oracle import oracle as O
+    n, depth = args.qubits, args.depth
+    c = W.scale_circuit(seed=2, n=n, depth=depth, keep=min(10, n))
+    if not O.have_reference():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference module not built (oracle/_ref)"}))
+        return
+    times, threads = reference_timings(n, c, args.steps, warm=args.warmup)
+    gates_per_layer = len(c.ops) / c.depth
+    per_gate = statistics.mean(times)
+    value = 1.0 / (per_gate * gates_per_layer)
+    sample = (f"one workload gate per step on {n} qubits (layer-0 U3 low/high, CNOT/CZ), "
+              f"layers/s = 1 / (mean s/gate x {gates_per_layer:.1f} gates/layer)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_gate * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(n, depth, c),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+    else:
+        engine_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,165 @@
+/*
+ * Internal structures of the B200 state-vector engine (not part of the ABI).
+ *
+ * Host side: immutable logical registers (dk_state) over reference-counted
+ * device buffers (dk_buf) with a persistent list of pending gates (dk_op).
+ * Device side: one amplitude array + a small scalar block per buffer.
+ */
+#ifndef DK_INTERNAL_H_
+#define DK_INTERNAL_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "dokigpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Largest gate the fused sweep executes in registers; larger gates go to the
+ * generic kernel (any k <= DK_MAX_GATE_QUBITS). */
+#define DK_SWEEP_MAX_K 3
+#define DK_MAX_GATE_QUBITS 10
+
+/* Per-buffer device scalars.  Logical amplitude = amp / norm.  csq is the
+ * exact sum of |amp|^2 of the stored content (kept so that sweeps which skip
+ * inactive tiles can still produce the reference's renormalisation). */
+typedef struct dk_scal {
+	double norm;
+	double csq;
+	double p_sel; /* last collapse: probability of the selected outcome */
+	double pad;
+	int32_t flag; /* last collapse: outcome (0/1) */
+	int32_t zero_norm; /* set when a collapse produced norm 0 */
+	int32_t pad2[2];
+} dk_scal;
+
+struct dk_gate {
+	int refcount;
+	unsigned k;
+	uint64_t dim;
+	double *m; /* host, 2 * dim * dim, row-major interleaved */
+};
+
+typedef struct dk_buf {
+	int refcount; /* logical registers sharing this storage */
+	unsigned n;
+	int prec;
+	void *d; /* amplitudes */
+	size_t bytes;
+	dk_scal *sc; /* device scalars */
+} dk_buf;
+
+typedef struct dk_op {
+	int refcount;
+	struct dk_op *prev; /* the op applied before this one (NULL = buffer) */
+	struct dk_gate *gate;
+	unsigned k;
+	unsigned tg[DK_MAX_GATE_QUBITS];
+	uint64_t cm, am;
+	uint32_t depth; /* chain length including this op */
+} dk_op;
+
+struct dk_state {
+	unsigned n;
+	int prec;
+	int released;
+	dk_buf *buf; /* NULL for 0-qubit registers */
+	dk_op *pending; /* ops queued on top of buf's content */
+	/* caches, valid while pending == NULL (a flushed register never changes) */
+	int have_norm;
+	double norm, csq;
+	int have_marg;
+	double *marg; /* n marginal sums S_q (raw content), host */
+	int have_phase;
+	double phase;
+	double *hcache; /* logical amplitudes (complex128), small registers */
+};
+
+/* ---- fused sweep program (built on the host, read by the sweep kernel) -- */
+
+#define DK_TILE_BITS_C128 12
+#define DK_TILE_BITS_C64 12
+#define DK_PASS_BITS 3
+
+enum {
+	DK_GK_DENSE1 = 1,
+	DK_GK_DIAG1 = 2,
+	DK_GK_ANTI1 = 3,
+	DK_GK_DENSE2 = 4,
+	DK_GK_DENSE3 = 5,
+	DK_GK_DIAGK = 6,
+};
+
+typedef struct dk_gate_desc {
+	uint8_t kind, k, t0, t1, t2, pad0, pad1, pad2; /* t_m: register bit of gate bit m */
+	uint32_t lc, la; /* control / anticontrol masks over local (tile) bits */
+	uint64_t gc, ga; /* control / anticontrol masks over global bits */
+	uint32_t mat; /* offset of the matrix in complex entries */
+	uint32_t pad3;
+} dk_gate_desc; /* 40 bytes */
+
+typedef struct dk_pass_desc {
+	uint8_t b[DK_PASS_BITS]; /* local bit of register bit j */
+	uint8_t nlane;
+	uint8_t lane[16]; /* local bit of thread-index bit j */
+	uint16_t g0, g1; /* gate range [g0, g1) */
+	uint32_t pad;
+} dk_pass_desc; /* 28 bytes -> padded */
+
+typedef struct dk_sweep_hdr {
+	int32_t m; /* tile bits */
+	int32_t n; /* register qubits */
+	int32_t npass, ngate;
+	int32_t all_touched; /* every tile has an unconditionally active gate */
+	int32_t pad;
+	uint64_t ntiles;
+	uint8_t qpos[16]; /* global bit of local bit j (ascending) */
+	uint32_t pass_off, gate_off, mat_off; /* byte offsets from the header */
+	uint32_t bytes; /* total program bytes */
+} dk_sweep_hdr;
+
+/* One step of a flush plan. */
+typedef struct dk_step {
+	int kind; /* 1 = fused sweep, 2 = generic single gate */
+	size_t prog_off; /* sweep: offset of its program in the plan blob */
+	int op_index; /* generic: index into the flat op array */
+	int ngates;
+} dk_step;
+
+typedef struct dk_flat_op {
+	const struct dk_gate *gate;
+	unsigned k;
+	unsigned tg[DK_MAX_GATE_QUBITS];
+	uint64_t cm, am;
+} dk_flat_op;
+
+typedef struct dk_plan {
+	dk_step *steps;
+	int nsteps;
+	unsigned char *blob; /* concatenated sweep programs (8-byte aligned) */
+	size_t blob_bytes;
+} dk_plan;
+
+/* Planner limits (per sweep). */
+typedef struct dk_plan_limits {
+	int tile_bits; /* m */
+	int low_bits; /* low qubits always in the tile (coalescing) */
+	int max_gates;
+	int max_passes;
+	int max_mat; /* complex entries */
+	int fuse; /* 0: one gate per sweep */
+} dk_plan_limits;
+
+void dk_plan_default_limits(int prec, unsigned n, dk_plan_limits *lim);
+int dk_plan_build(const dk_flat_op *ops, int nops, unsigned n, int prec,
+		  const dk_plan_limits *lim, dk_plan *plan);
+void dk_plan_free(dk_plan *plan);
+int dk_gate_classify(const struct dk_gate *g);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DK_INTERNAL_H_ */

@@ -1,0 +1,1161 @@
+/*
+ * CUDA kernels of the B200 state-vector engine (sm_100a).
+ *
+ * Amplitudes are complex128 (double2) or complex64 (float2), 16 / 8 bytes,
+ * qubit q = bit q of the index.  Every reduction is FP64 and deterministic:
+ * blocks write partial sums into a scratch array and a single-block
+ * finalize kernel adds them in a fixed order.
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "dk_kernels.h"
+
+namespace dk {
+namespace {
+
+template <typename R> struct CT;
+template <> struct CT<double> {
+	typedef double2 T;
+};
+template <> struct CT<float> {
+	typedef float2 T;
+};
+
+__device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ float2 mk(float x, float y) { return make_float2(x, y); }
+
+template <typename C2> __device__ __forceinline__ C2 ldm(const double2 *p);
+template <> __device__ __forceinline__ double2 ldm<double2>(const double2 *p) { return __ldg(p); }
+template <> __device__ __forceinline__ float2 ldm<float2>(const double2 *p)
+{
+	double2 v = __ldg(p);
+	return make_float2((float)v.x, (float)v.y);
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+	return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+	return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+/* a * b + c */
+__device__ __forceinline__ double2 cmad(double2 a, double2 b, double2 c)
+{
+	return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)),
+			    fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ float2 cmad(float2 a, float2 b, float2 c)
+{
+	return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)),
+			   fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ double sqabs(double2 a) { return fma(a.x, a.x, a.y * a.y); }
+__device__ __forceinline__ double sqabs(float2 a)
+{
+	double x = a.x, y = a.y;
+	return fma(x, x, y * y);
+}
+__device__ __forceinline__ double2 to_c128(double2 a) { return a; }
+__device__ __forceinline__ double2 to_c128(float2 a) { return make_double2(a.x, a.y); }
+template <typename C2> __device__ __forceinline__ C2 from_c128(double2 a);
+template <> __device__ __forceinline__ double2 from_c128<double2>(double2 a) { return a; }
+template <> __device__ __forceinline__ float2 from_c128<float2>(double2 a)
+{
+	return make_float2((float)a.x, (float)a.y);
+}
+
+/* XOR swizzle of the shared tile: the low SW bits of the slot are XORed with
+ * every higher SW-bit group, so any SW thread bits mapped to tile bits of
+ * distinct residues mod SW hit distinct 16-byte (8-byte) bank groups. */
+template <int SW> __device__ __forceinline__ uint32_t swz(uint32_t i)
+{
+	uint32_t f = 0;
+#pragma unroll
+	for (int s = SW; s < 20; s += SW)
+		f ^= i >> s;
+	return i ^ (f & ((1u << SW) - 1u));
+}
+
+__device__ __forceinline__ bool ctl_ok(uint32_t loc, uint32_t lc, uint32_t la)
+{
+	return ((loc & lc) == lc) && !(loc & la);
+}
+
+/* ---- gate application on the 8 register amplitudes of a pass ------------
+ * a[r] holds the amplitude whose pass bits equal r; loc[r] is its tile
+ * index (for local control predicates).  t_m: register bit of gate bit m. */
+
+template <int T, typename C2>
+__device__ __forceinline__ void g_dense1(C2 (&a)[8], const uint32_t (&loc)[8],
+					 uint32_t lc, uint32_t la, const double2 *mt)
+{
+	const C2 m00 = ldm<C2>(mt), m01 = ldm<C2>(mt + 1);
+	const C2 m10 = ldm<C2>(mt + 2), m11 = ldm<C2>(mt + 3);
+#pragma unroll
+	for (int r = 0; r < 8; ++r) {
+		if (r & (1 << T))
+			continue;
+		const int r1 = r | (1 << T);
+		if (ctl_ok(loc[r], lc, la)) {
+			const C2 x = a[r], y = a[r1];
+			a[r] = cmad(m01, y, cmul(m00, x));
+			a[r1] = cmad(m11, y, cmul(m10, x));
+		}
+	}
+}
+
+template <int T, typename C2>
+__device__ __forceinline__ void g_anti1(C2 (&a)[8], const uint32_t (&loc)[8],
+					uint32_t lc, uint32_t la, const double2 *mt)
+{
+	const C2 m01 = ldm<C2>(mt), m10 = ldm<C2>(mt + 1);
+#pragma unroll
+	for (int r = 0; r < 8; ++r) {
+		if (r & (1 << T))
+			continue;
+		const int r1 = r | (1 << T);
+		if (ctl_ok(loc[r], lc, la)) {
+			const C2 x = a[r], y = a[r1];
+			a[r] = cmul(m01, y);
+			a[r1] = cmul(m10, x);
+		}
+	}
+}
+
+template <typename C2>
+__device__ __forceinline__ void g_diag1(C2 (&a)[8], const uint32_t (&loc)[8],
+					uint32_t lc, uint32_t la, int t,
+					const double2 *mt)
+{
+	const C2 d0 = ldm<C2>(mt), d1 = ldm<C2>(mt + 1);
+#pragma unroll
+	for (int r = 0; r < 8; ++r)
+		if (ctl_ok(loc[r], lc, la))
+			a[r] = cmul(((r >> t) & 1) ? d1 : d0, a[r]);
+}
+
+template <typename C2>
+__device__ __forceinline__ void g_diagk(C2 (&a)[8], const uint32_t (&loc)[8],
+					uint32_t lc, uint32_t la, int k, int t0,
+					int t1, int t2, const double2 *mt)
+{
+#pragma unroll
+	for (int r = 0; r < 8; ++r) {
+		int gi = (r >> t0) & 1;
+		if (k > 1)
+			gi |= ((r >> t1) & 1) << 1;
+		if (k > 2)
+			gi |= ((r >> t2) & 1) << 2;
+		if (ctl_ok(loc[r], lc, la))
+			a[r] = cmul(ldm<C2>(mt + gi), a[r]);
+	}
+}
+
+template <int T0, int T1, typename C2>
+__device__ __forceinline__ void g_dense2(C2 (&a)[8], const uint32_t (&loc)[8],
+					 uint32_t lc, uint32_t la, const double2 *mt)
+{
+	constexpr int R = 3 - T0 - T1;
+#pragma unroll
+	for (int h = 0; h < 2; ++h) {
+		const int b = h << R;
+		const int i0 = b, i1 = b | (1 << T0), i2 = b | (1 << T1),
+			  i3 = b | (1 << T0) | (1 << T1);
+		if (!ctl_ok(loc[b], lc, la))
+			continue;
+		const C2 x0 = a[i0], x1 = a[i1], x2 = a[i2], x3 = a[i3];
+		C2 y[4];
+#pragma unroll
+		for (int row = 0; row < 4; ++row) {
+			C2 s = cmul(ldm<C2>(mt + 4 * row), x0);
+			s = cmad(ldm<C2>(mt + 4 * row + 1), x1, s);
+			s = cmad(ldm<C2>(mt + 4 * row + 2), x2, s);
+			y[row] = cmad(ldm<C2>(mt + 4 * row + 3), x3, s);
+		}
+		a[i0] = y[0];
+		a[i1] = y[1];
+		a[i2] = y[2];
+		a[i3] = y[3];
+	}
+}
+
+template <int T0, int T1, int T2, typename C2>
+__device__ __forceinline__ void g_dense3(C2 (&a)[8], const uint32_t (&loc)[8],
+					 uint32_t lc, uint32_t la, const double2 *mt)
+{
+	if (!ctl_ok(loc[0], lc, la))
+		return;
+	C2 x[8];
+#pragma unroll
+	for (int g = 0; g < 8; ++g)
+		x[g] = a[((g & 1) << T0) | (((g >> 1) & 1) << T1) | ((g >> 2) << T2)];
+#pragma unroll
+	for (int row = 0; row < 8; ++row) {
+		C2 s = cmul(ldm<C2>(mt + 8 * row), x[0]);
+#pragma unroll
+		for (int c = 1; c < 8; ++c)
+			s = cmad(ldm<C2>(mt + 8 * row + c), x[c], s);
+		a[((row & 1) << T0) | (((row >> 1) & 1) << T1) | ((row >> 2) << T2)] = s;
+	}
+}
+
+template <typename C2>
+__device__ __forceinline__ void g_dense3_any(C2 (&a)[8], const uint32_t (&loc)[8],
+					  uint32_t lc, uint32_t la, int t0, int t1,
+					  const double2 *mt)
+{
+	/* t2 is implied: the three register bits are a permutation */
+	if (t0 == 0 && t1 == 1)
+		g_dense3<0, 1, 2>(a, loc, lc, la, mt);
+	else if (t0 == 0)
+		g_dense3<0, 2, 1>(a, loc, lc, la, mt);
+	else if (t0 == 1 && t1 == 0)
+		g_dense3<1, 0, 2>(a, loc, lc, la, mt);
+	else if (t0 == 1)
+		g_dense3<1, 2, 0>(a, loc, lc, la, mt);
+	else if (t1 == 0)
+		g_dense3<2, 0, 1>(a, loc, lc, la, mt);
+	else
+		g_dense3<2, 1, 0>(a, loc, lc, la, mt);
+}
+
+template <typename C2>
+__device__ __forceinline__ void apply_gate(C2 (&a)[8], const uint32_t (&loc)[8],
+					   const dk_gate_desc &gd, const double2 *mats)
+{
+	const double2 *mt = mats + gd.mat;
+	const uint32_t lc = gd.lc, la = gd.la;
+	switch (gd.kind) {
+	case DK_GK_DENSE1:
+		if (gd.t0 == 0)
+			g_dense1<0>(a, loc, lc, la, mt);
+		else if (gd.t0 == 1)
+			g_dense1<1>(a, loc, lc, la, mt);
+		else
+			g_dense1<2>(a, loc, lc, la, mt);
+		break;
+	case DK_GK_ANTI1:
+		if (gd.t0 == 0)
+			g_anti1<0>(a, loc, lc, la, mt);
+		else if (gd.t0 == 1)
+			g_anti1<1>(a, loc, lc, la, mt);
+		else
+			g_anti1<2>(a, loc, lc, la, mt);
+		break;
+	case DK_GK_DIAG1:
+		g_diag1(a, loc, lc, la, gd.t0, mt);
+		break;
+	case DK_GK_DIAGK:
+		g_diagk(a, loc, lc, la, gd.k, gd.t0, gd.t1, gd.t2, mt);
+		break;
+	case DK_GK_DENSE2: {
+		const int c = gd.t0 * 3 + gd.t1;
+		switch (c) {
+		case 1: g_dense2<0, 1>(a, loc, lc, la, mt); break;
+		case 2: g_dense2<0, 2>(a, loc, lc, la, mt); break;
+		case 3: g_dense2<1, 0>(a, loc, lc, la, mt); break;
+		case 5: g_dense2<1, 2>(a, loc, lc, la, mt); break;
+		case 6: g_dense2<2, 0>(a, loc, lc, la, mt); break;
+		default: g_dense2<2, 1>(a, loc, lc, la, mt); break;
+		}
+		break;
+	}
+	case DK_GK_DENSE3:
+		g_dense3_any(a, loc, lc, la, gd.t0, gd.t1, mt);
+		break;
+	default:
+		break;
+	}
+}
+
+/* block-wide sum of two doubles; result valid in thread 0 */
+__device__ __forceinline__ void block_sum2(double &x, double &y)
+{
+	__shared__ double red[2][32];
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		x += __shfl_xor_sync(0xffffffffu, x, o);
+		y += __shfl_xor_sync(0xffffffffu, y, o);
+	}
+	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+	if (l == 0) {
+		red[0][w] = x;
+		red[1][w] = y;
+	}
+	__syncthreads();
+	const int nw = (blockDim.x + 31) >> 5;
+	if (w == 0) {
+		x = l < nw ? red[0][l] : 0.0;
+		y = l < nw ? red[1][l] : 0.0;
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			x += __shfl_xor_sync(0xffffffffu, x, o);
+			y += __shfl_xor_sync(0xffffffffu, y, o);
+		}
+	}
+	__syncthreads();
+}
+
+/* ---- fused sweep ------------------------------------------------------- */
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+	const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+	const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+	asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+/* One CTA per SM streams tiles of 2^m amplitudes (index bits = the sweep's
+ * qubit set, lowest qubits first so each tile is made of contiguous runs)
+ * through two shared-memory buffers: while tile t is processed, tile t+grid
+ * is already being copied in with cp.async.  Each pass gathers 8 amplitudes
+ * per thread (the 3 pass bits) into registers, applies the pass's gates and
+ * scatters them back; the last read-out streams the tile to `out`.  The sum
+ * of |amp|^2 read (touched tiles) and written goes to per-block partials. */
+template <typename R, int M, int SW>
+__global__ void __launch_bounds__(1 << (M - 3), 1)
+	k_sweep(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
+		const unsigned char *__restrict__ prog, double *partials)
+{
+	typedef typename CT<R>::T C2;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const dk_sweep_hdr *h = reinterpret_cast<const dk_sweep_hdr *>(prog);
+	const int m = h->m;
+	const int lanes = m - 3;
+	const uint32_t tid = threadIdx.x;
+	const int npass = h->npass, ngate = h->ngate;
+	const size_t tile_bytes = (size_t)sizeof(C2) << m;
+	const size_t pass_bytes = ((size_t)npass * sizeof(dk_pass_desc) + 15) & ~(size_t)15;
+	C2 *buf0 = reinterpret_cast<C2 *>(sm);
+	C2 *buf1 = reinterpret_cast<C2 *>(sm + tile_bytes);
+	dk_pass_desc *sp = reinterpret_cast<dk_pass_desc *>(sm + 2 * tile_bytes);
+	dk_gate_desc *sg = reinterpret_cast<dk_gate_desc *>(sm + 2 * tile_bytes + pass_bytes);
+	__shared__ uint8_t sq[16];
+
+	{ /* stage the pass / gate tables and the tile bit positions */
+		const uint32_t *src = reinterpret_cast<const uint32_t *>(prog + h->pass_off);
+		uint32_t *dst = reinterpret_cast<uint32_t *>(sp);
+		const int nw = (int)(npass * sizeof(dk_pass_desc) / 4);
+		for (int i = tid; i < nw; i += blockDim.x)
+			dst[i] = __ldg(src + i);
+		src = reinterpret_cast<const uint32_t *>(prog + h->gate_off);
+		dst = reinterpret_cast<uint32_t *>(sg);
+		const int gw = (int)(ngate * sizeof(dk_gate_desc) / 4);
+		for (int i = tid; i < gw; i += blockDim.x)
+			dst[i] = __ldg(src + i);
+		if (tid < 16)
+			sq[tid] = h->qpos[tid];
+	}
+	__syncthreads();
+	const double2 *mats = reinterpret_cast<const double2 *>(prog + h->mat_off);
+
+	uint64_t off_t = 0;
+	for (int j = 0; j < lanes; ++j)
+		if ((tid >> j) & 1u)
+			off_t |= 1ull << sq[j];
+	const uint64_t h0 = 1ull << sq[lanes], h1 = 1ull << sq[lanes + 1],
+		       h2 = 1ull << sq[lanes + 2];
+	const uint64_t ntiles = h->ntiles;
+	const bool skip_idle = (in == out) && !h->all_touched;
+
+	auto tile_base = [&](uint64_t t) -> uint64_t {
+		uint64_t base = t;
+		for (int j = 0; j < m; ++j) {
+			const int q = sq[j];
+			base = ((base >> q) << (q + 1)) | (base & ((1ull << q) - 1ull));
+		}
+		return base;
+	};
+	/* next tile (>= t, stepping by the grid) with at least one active gate */
+	auto next_tile = [&](uint64_t t) -> uint64_t {
+		for (; t < ntiles; t += gridDim.x) {
+			if (!skip_idle)
+				return t;
+			const uint64_t base = tile_base(t);
+			for (int g = 0; g < ngate; ++g)
+				if (((base & sg[g].gc) == sg[g].gc) && !(base & sg[g].ga))
+					return t;
+		}
+		return ntiles;
+	};
+	auto prefetch = [&](uint64_t t, C2 *buf) {
+		const uint64_t base = tile_base(t) | off_t;
+#pragma unroll
+		for (int r = 0; r < 8; ++r) {
+			const uint64_t gi = base | ((r & 1) ? h0 : 0) | ((r & 2) ? h1 : 0) |
+					    ((r & 4) ? h2 : 0);
+			C2 *dst = buf + swz<SW>(tid + ((uint32_t)r << lanes));
+			if (sizeof(C2) == 16)
+				cp_async16(dst, in + gi);
+			else
+				cp_async8(dst, in + gi);
+		}
+		cp_async_commit();
+	};
+
+	double insq = 0.0, outsq = 0.0;
+	uint64_t t = next_tile(blockIdx.x);
+	if (t < ntiles)
+		prefetch(t, buf0);
+	int cur = 0;
+	while (t < ntiles) {
+		const uint64_t base = tile_base(t);
+		const uint64_t tn = next_tile(t + gridDim.x);
+		C2 *tile = cur ? buf1 : buf0;
+		if (tn < ntiles) {
+			prefetch(tn, cur ? buf0 : buf1);
+			cp_async_wait<1>();
+		} else {
+			cp_async_wait<0>();
+		}
+		__syncthreads();
+		C2 a[8];
+		for (int p = 0; p < npass; ++p) {
+			const dk_pass_desc &pd = sp[p];
+			uint32_t gb = 0;
+			for (int j = 0; j < lanes; ++j)
+				gb |= ((tid >> j) & 1u) << pd.lane[j];
+			const uint32_t p0 = 1u << pd.b[0], p1 = 1u << pd.b[1],
+				       p2 = 1u << pd.b[2];
+			uint32_t loc[8];
+#pragma unroll
+			for (int r = 0; r < 8; ++r)
+				loc[r] = gb | ((r & 1) ? p0 : 0) | ((r & 2) ? p1 : 0) |
+					 ((r & 4) ? p2 : 0);
+#pragma unroll
+			for (int r = 0; r < 8; ++r)
+				a[r] = tile[swz<SW>(loc[r])];
+			if (p == 0) {
+#pragma unroll
+				for (int r = 0; r < 8; ++r)
+					insq += sqabs(a[r]);
+			}
+			const int g1 = pd.g1;
+			for (int g = pd.g0; g < g1; ++g) {
+				const dk_gate_desc &gd = sg[g];
+				if (((base & gd.gc) != gd.gc) || (base & gd.ga))
+					continue;
+				apply_gate(a, loc, gd, mats);
+			}
+#pragma unroll
+			for (int r = 0; r < 8; ++r)
+				tile[swz<SW>(loc[r])] = a[r];
+			__syncthreads();
+		}
+#pragma unroll
+		for (int r = 0; r < 8; ++r)
+			a[r] = tile[swz<SW>(tid + ((uint32_t)r << lanes))];
+		__syncthreads(); /* the buffer is refilled by the next prefetch */
+		const uint64_t bo = base | off_t;
+#pragma unroll
+		for (int r = 0; r < 8; ++r) {
+			const uint64_t gi = bo | ((r & 1) ? h0 : 0) | ((r & 2) ? h1 : 0) |
+					    ((r & 4) ? h2 : 0);
+			outsq += sqabs(a[r]);
+			__stcs(out + gi, a[r]);
+		}
+		t = tn;
+		cur ^= 1;
+	}
+	cp_async_wait<0>();
+	block_sum2(insq, outsq);
+	if (tid == 0) {
+		partials[2 * blockIdx.x] = insq;
+		partials[2 * blockIdx.x + 1] = outsq;
+	}
+}
+
+enum { FIN_GATE = 0, FIN_COLLAPSE = 1, FIN_RESET = 2 };
+
+/* Sum the (in, out) partials of `nb` blocks in a fixed order and update the
+ * output scalars.  FIN_GATE: csq = all ? out : csq_in - in + out, norm =
+ * sqrt(csq).  FIN_COLLAPSE: csq = out, norm = norm_in * sqrt(p_sel).
+ * FIN_RESET: csq = out, norm = 1. */
+__global__ void k_finalize(const double *partials, int nb, const dk_scal *sc_in,
+			   dk_scal *sc_out, int mode, int all)
+{
+	__shared__ double sx[256], sy[256];
+	double x = 0.0, y = 0.0;
+	for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+		x += partials[2 * i];
+		y += partials[2 * i + 1];
+	}
+	sx[threadIdx.x] = x;
+	sy[threadIdx.x] = y;
+	__syncthreads();
+	for (int s = blockDim.x >> 1; s > 0; s >>= 1) {
+		if ((int)threadIdx.x < s) {
+			sx[threadIdx.x] += sx[threadIdx.x + s];
+			sy[threadIdx.x] += sy[threadIdx.x + s];
+		}
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) {
+		const double sin_ = sx[0], sout = sy[0];
+		if (mode == FIN_GATE) {
+			const double c = all ? sout : (sc_in->csq - sin_ + sout);
+			sc_out->csq = c;
+			sc_out->norm = sqrt(c);
+		} else if (mode == FIN_COLLAPSE) {
+			const double nrm = sc_in->norm * sqrt(sc_out->p_sel);
+			sc_out->csq = sout;
+			sc_out->norm = nrm;
+			if (nrm == 0.0)
+				sc_out->zero_norm = 1;
+		} else {
+			sc_out->csq = sout;
+			sc_out->norm = 1.0;
+		}
+	}
+}
+
+/* ---- generic single gate (any k), out of place ----------------------- */
+
+struct GenTargets {
+	uint8_t t[DK_MAX_GATE_QUBITS];
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_generic(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
+		  uint64_t size, int k, GenTargets tg, uint64_t cm, uint64_t am,
+		  const double2 *__restrict__ mat, double *partials)
+{
+	typedef typename CT<R>::T C2;
+	uint64_t tmask = 0;
+	for (int j = 0; j < k; ++j)
+		tmask |= 1ull << tg.t[j];
+	const uint32_t dim = 1u << k;
+	double outsq = 0.0, dummy = 0.0;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < size;
+	     i += (uint64_t)gridDim.x * blockDim.x) {
+		C2 v;
+		if ((i & cm) == cm && !(i & am)) {
+			uint32_t row = 0;
+			for (int j = 0; j < k; ++j)
+				row |= (uint32_t)((i >> tg.t[j]) & 1u) << j;
+			const uint64_t clr = i & ~tmask;
+			double2 acc = make_double2(0.0, 0.0);
+			for (uint32_t col = 0; col < dim; ++col) {
+				uint64_t src = clr;
+				for (int j = 0; j < k; ++j)
+					src |= (uint64_t)((col >> j) & 1u) << tg.t[j];
+				acc = cmad(__ldg(mat + (uint64_t)row * dim + col),
+					   to_c128(in[src]), acc);
+			}
+			v = from_c128<C2>(acc);
+		} else {
+			v = in[i];
+		}
+		out[i] = v;
+		outsq += sqabs(v);
+	}
+	block_sum2(dummy, outsq);
+	if (threadIdx.x == 0) {
+		partials[2 * blockIdx.x] = 0.0;
+		partials[2 * blockIdx.x + 1] = outsq;
+	}
+}
+
+/* ---- initialisation / import ------------------------------------------ */
+
+template <typename R>
+__global__ void k_set_one(typename CT<R>::T *d, dk_scal *sc)
+{
+	d[0] = mk((R)1, (R)0);
+	sc->norm = 1.0;
+	sc->csq = 1.0;
+	sc->p_sel = 0.0;
+	sc->flag = 0;
+	sc->zero_norm = 0;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_import(const double2 *__restrict__ src, typename CT<R>::T *dst,
+		 uint64_t size, double *partials)
+{
+	typedef typename CT<R>::T C2;
+	double s = 0.0, dummy = 0.0;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < size;
+	     i += (uint64_t)gridDim.x * blockDim.x) {
+		const C2 v = from_c128<C2>(src[i]);
+		dst[i] = v;
+		s += sqabs(v);
+	}
+	block_sum2(dummy, s);
+	if (threadIdx.x == 0) {
+		partials[2 * blockIdx.x] = 0.0;
+		partials[2 * blockIdx.x + 1] = s;
+	}
+}
+
+__global__ void k_clear_flags(dk_scal *sc)
+{
+	sc->zero_norm = 0;
+	sc->flag = 0;
+	sc->p_sel = 0.0;
+}
+
+/* ---- marginals: S_q = sum_{bit q of i set} |amp_i|^2 for all q --------
+ * Thread g visits i = (k << s) | g, s = log2(total threads): bits below s are
+ * fixed per thread, bits above vary with k and are accumulated per bit. */
+constexpr int kMargHi = 24;
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_marginals(const typename CT<R>::T *__restrict__ d, int n, int s,
+		    double *partials)
+{
+	const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	const int nb = n - s;
+	const uint64_t cnt = 1ull << nb;
+	double tot = 0.0;
+	double hi[kMargHi];
+#pragma unroll
+	for (int j = 0; j < kMargHi; ++j)
+		hi[j] = 0.0;
+	for (uint64_t k = 0; k < cnt; ++k) {
+		const double p = sqabs(__ldcs(d + ((k << s) | g)));
+		tot += p;
+#pragma unroll
+		for (int j = 0; j < kMargHi; ++j)
+			if (j < nb && ((k >> j) & 1u))
+				hi[j] += p;
+	}
+	__shared__ double red[32];
+	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+	const int nw = blockDim.x >> 5;
+	/* values to reduce: q < s -> tot * bit_q(g); q = s + j -> hi[j]; q = n -> tot */
+	for (int q = 0; q <= n; ++q) {
+		double v;
+		if (q == n)
+			v = tot;
+		else if (q < s)
+			v = ((g >> q) & 1u) ? tot : 0.0;
+		else {
+			v = 0.0;
+#pragma unroll
+			for (int j = 0; j < kMargHi; ++j)
+				if (j == q - s)
+					v = hi[j];
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1)
+			v += __shfl_xor_sync(0xffffffffu, v, o);
+		if (l == 0)
+			red[w] = v;
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double t = 0.0;
+			for (int i = 0; i < nw; ++i)
+				t += red[i];
+			partials[(size_t)blockIdx.x * kPartialStride + q] = t;
+		}
+		__syncthreads();
+	}
+}
+
+__global__ void k_marg_finalize(const double *partials, int nb, int n, double *marg)
+{
+	const int q = threadIdx.x;
+	if (q > n)
+		return;
+	double t = 0.0;
+	for (int b = 0; b < nb; ++b)
+		t += partials[(size_t)b * kPartialStride + q];
+	marg[q] = t;
+}
+
+/* ---- measurement -------------------------------------------------------- */
+
+/* qops.c:124-136: P(1) = S_q / norm^2 (the reference sums |amp/norm|^2);
+ * result = P(1) > roll (or the forced value); keep the selected probability. */
+__global__ void k_decide(const double *marg, int q, double roll, int forced,
+			 const dk_scal *sc_in, dk_scal *sc_out)
+{
+	const double nrm = sc_in->norm;
+	const double p1 = marg[q] / (nrm * nrm);
+	const int res = forced >= 0 ? forced : (p1 > roll ? 1 : 0);
+	sc_out->flag = res;
+	sc_out->p_sel = res ? p1 : 1.0 - p1;
+}
+
+/* qops.c:138-174: out[j] = in[insert bit q = outcome into j] */
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_collapse(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
+		   uint64_t half, int q, const dk_scal *sc_sel, double *partials)
+{
+	typedef typename CT<R>::T C2;
+	const uint64_t v = (uint64_t)sc_sel->flag << q;
+	const uint64_t low = (1ull << q) - 1ull;
+	double s = 0.0, dummy = 0.0;
+	for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < half;
+	     j += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t i = ((j & ~low) << 1) | v | (j & low);
+		const C2 x = __ldcs(in + i);
+		__stcs(out + j, x);
+		s += sqabs(x);
+	}
+	block_sum2(dummy, s);
+	if (threadIdx.x == 0) {
+		partials[2 * blockIdx.x] = 0.0;
+		partials[2 * blockIdx.x + 1] = s;
+	}
+}
+
+/* ---- join (qops.c:97-122) ---------------------------------------------- */
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_join(const typename CT<R>::T *__restrict__ most, const dk_scal *sc1,
+	       const typename CT<R>::T *__restrict__ least, const dk_scal *sc2,
+	       int n2, typename CT<R>::T *out, uint64_t size, double *partials)
+{
+	typedef typename CT<R>::T C2;
+	const double i1 = 1.0 / sc1->norm, i2 = 1.0 / sc2->norm;
+	const uint64_t lm = (1ull << n2) - 1ull;
+	double s = 0.0, dummy = 0.0;
+	for (uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; o < size;
+	     o += (uint64_t)gridDim.x * blockDim.x) {
+		const double2 a = to_c128(most[o >> n2]);
+		const double2 b = to_c128(__ldg(least + (o & lm)));
+		const double2 an = make_double2(a.x * i1, a.y * i1);
+		const double2 bn = make_double2(b.x * i2, b.y * i2);
+		const C2 v = from_c128<C2>(cmul(an, bn));
+		__stcs(out + o, v);
+		s += sqabs(v);
+	}
+	block_sum2(dummy, s);
+	if (threadIdx.x == 0) {
+		partials[2 * blockIdx.x] = 0.0;
+		partials[2 * blockIdx.x + 1] = s;
+	}
+}
+
+/* ---- first non-zero amplitude (qops.c:57-65) ---------------------------- */
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_first_nz(const typename CT<R>::T *__restrict__ d, uint64_t first,
+		   uint64_t count, unsigned long long *res)
+{
+	unsigned long long best = ~0ull;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+	     i += (uint64_t)gridDim.x * blockDim.x) {
+		const typename CT<R>::T v = d[first + i];
+		if (v.x != 0 || v.y != 0) {
+			best = first + i;
+			break; /* later i of this thread are larger */
+		}
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
+		best = x < best ? x : best;
+	}
+	if ((threadIdx.x & 31) == 0 && best != ~0ull)
+		atomicMin(res, best);
+}
+
+/* ---- reduced density matrix helpers ------------------------------------ */
+__device__ __forceinline__ uint64_t deposit(uint64_t v, uint64_t mask)
+{
+	uint64_t r = 0;
+	for (uint64_t b = 1; mask; b <<= 1) {
+		const uint64_t low = mask & (~mask + 1ull);
+		if (v & b)
+			r |= low;
+		mask &= mask - 1ull;
+	}
+	return r;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_gather_kept(const typename CT<R>::T *__restrict__ d, uint64_t keep,
+		      uint64_t trace, int k, uint64_t total, double2 *M)
+{
+	for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+	     e += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t a = e & ((1ull << k) - 1ull), b = e >> k;
+		M[e] = to_c128(d[deposit(a, keep) | deposit(b, trace)]);
+	}
+}
+
+__global__ void __launch_bounds__(256)
+	k_herm_fill(const double2 *__restrict__ C, double2 *rho, uint64_t dim)
+{
+	const uint64_t total = dim * dim;
+	for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+	     e += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t a = e / dim, a2 = e % dim;
+		double2 v;
+		if (a >= a2)
+			v = C[a + a2 * dim];
+		else {
+			v = C[a2 + a * dim];
+			v.y = -v.y;
+		}
+		rho[e] = v;
+	}
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_rho_elem(const typename CT<R>::T *__restrict__ d, uint64_t ia, uint64_t ib,
+		   uint64_t trace, uint64_t cnt, double *partials)
+{
+	double re = 0.0, im = 0.0;
+	for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < cnt;
+	     b += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t off = deposit(b, trace);
+		const double2 x = to_c128(d[ia | off]), y = to_c128(d[ib | off]);
+		/* x * conj(y) */
+		re += x.x * y.x + x.y * y.y;
+		im += x.y * y.x - x.x * y.y;
+	}
+	block_sum2(re, im);
+	if (threadIdx.x == 0) {
+		partials[2 * blockIdx.x] = re;
+		partials[2 * blockIdx.x + 1] = im;
+	}
+}
+
+__global__ void k_rho_elem_finalize(const double *partials, int nb,
+				    const dk_scal *sc, double *outv)
+{
+	if (threadIdx.x != 0)
+		return;
+	double re = 0.0, im = 0.0;
+	for (int b = 0; b < nb; ++b) {
+		re += partials[2 * b];
+		im += partials[2 * b + 1];
+	}
+	const double n2 = sc->norm * sc->norm;
+	outv[0] = re / n2;
+	outv[1] = im / n2;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_export(const typename CT<R>::T *__restrict__ d, uint64_t first,
+		 uint64_t count, double2 *dst)
+{
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+	     i += (uint64_t)gridDim.x * blockDim.x)
+		dst[i] = to_c128(d[first + i]);
+}
+
+__global__ void k_copy_scal(const dk_scal *a, dk_scal *b) { *b = *a; }
+
+inline int grid_for(uint64_t work, int per_block, int cap)
+{
+	uint64_t b = (work + per_block - 1) / per_block;
+	if (b < 1)
+		b = 1;
+	if (b > (uint64_t)cap)
+		b = cap;
+	return (int)b;
+}
+
+int g_num_sms = 148;
+
+} // namespace
+
+unsigned long long g_launches = 0;
+
+/* ---------------------------------------------------------------------- */
+
+cudaError_t launch_sweep(int prec, const void *in, void *out,
+			 const unsigned char *dprog, const dk_sweep_hdr *hp,
+			 const dk_scal *sc_in, dk_scal *sc_out, const Scratch &s,
+			 int num_sms, cudaStream_t st)
+{
+	g_num_sms = num_sms;
+	const int m = hp->m;
+	const int threads = 1 << (m - 3);
+	const size_t pass_bytes = ((size_t)hp->npass * sizeof(dk_pass_desc) + 15) & ~(size_t)15;
+	const size_t gate_bytes = (size_t)hp->ngate * sizeof(dk_gate_desc);
+	uint64_t blocks64 = hp->ntiles;
+	const uint64_t cap = (uint64_t)num_sms;
+	if (blocks64 > cap)
+		blocks64 = cap;
+	const int blocks = (int)blocks64;
+	cudaError_t e;
+	if (prec == DK_C128) {
+		const size_t smem = ((size_t)32 << m) + pass_bytes + gate_bytes;
+		auto kern = k_sweep<double, DK_TILE_BITS_C128, 3>;
+		e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+					 (int)smem);
+		if (e != cudaSuccess)
+			return e;
+		kern<<<blocks, threads, smem, st>>>((const double2 *)in, (double2 *)out,
+						   dprog, s.partials);
+	} else {
+		const size_t smem = ((size_t)16 << m) + pass_bytes + gate_bytes;
+		auto kern = k_sweep<float, DK_TILE_BITS_C64, 4>;
+		e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+					 (int)smem);
+		if (e != cudaSuccess)
+			return e;
+		kern<<<blocks, threads, smem, st>>>((const float2 *)in, (float2 *)out,
+						   dprog, s.partials);
+	}
+	const int all = hp->all_touched || (in != out);
+	k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc_in, sc_out, FIN_GATE, all);
+	g_launches += 2;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_generic_gate(int prec, const void *in, void *out, unsigned n,
+				unsigned k, const unsigned *tg, uint64_t cm,
+				uint64_t am, const double *dmat,
+				const dk_scal *sc_in, dk_scal *sc_out,
+				const Scratch &s, cudaStream_t st)
+{
+	GenTargets t;
+	for (unsigned j = 0; j < DK_MAX_GATE_QUBITS; ++j)
+		t.t[j] = j < k ? (uint8_t)tg[j] : 0;
+	const uint64_t size = 1ull << n;
+	const int blocks = grid_for(size, 256 * 4, g_num_sms * 8);
+	if (prec == DK_C128)
+		k_generic<double><<<blocks, 256, 0, st>>>(
+			(const double2 *)in, (double2 *)out, size, (int)k, t, cm, am,
+			(const double2 *)dmat, s.partials);
+	else
+		k_generic<float><<<blocks, 256, 0, st>>>(
+			(const float2 *)in, (float2 *)out, size, (int)k, t, cm, am,
+			(const double2 *)dmat, s.partials);
+	k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc_in, sc_out, FIN_GATE, 1);
+	g_launches += 2;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_init_zero(int prec, void *d, unsigned n, dk_scal *sc,
+			     cudaStream_t st)
+{
+	const size_t bytes = (prec == DK_C128 ? 16 : 8) * ((size_t)1 << n);
+	cudaError_t e = cudaMemsetAsync(d, 0, bytes, st);
+	if (e != cudaSuccess)
+		return e;
+	if (prec == DK_C128)
+		k_set_one<double><<<1, 1, 0, st>>>((double2 *)d, sc);
+	else
+		k_set_one<float><<<1, 1, 0, st>>>((float2 *)d, sc);
+	g_launches += 1;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_import(int prec, const double *src, void *d, unsigned n,
+			  dk_scal *sc, const Scratch &s, cudaStream_t st)
+{
+	const uint64_t size = 1ull << n;
+	const int blocks = grid_for(size, 256 * 4, g_num_sms * 8);
+	k_clear_flags<<<1, 1, 0, st>>>(sc);
+	if (prec == DK_C128)
+		k_import<double><<<blocks, 256, 0, st>>>((const double2 *)src,
+							(double2 *)d, size, s.partials);
+	else
+		k_import<float><<<blocks, 256, 0, st>>>((const double2 *)src,
+						       (float2 *)d, size, s.partials);
+	k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc, sc, FIN_RESET, 1);
+	g_launches += 3;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_marginals(int prec, const void *d, unsigned n, const Scratch &s,
+			     cudaStream_t st)
+{
+	int threads = 256, blocks = 1;
+	if (n < 8)
+		threads = 1 << n;
+	else {
+		int lb = (int)n - 8;
+		if (lb > 10)
+			lb = 10;
+		blocks = 1 << lb;
+	}
+	int sbits = 0;
+	while ((1 << sbits) < threads * blocks)
+		sbits++;
+	if ((int)n - sbits > kMargHi)
+		return cudaErrorInvalidValue;
+	if (threads < 32) {
+		/* tiny registers: one warp, lanes beyond the register are idle */
+		threads = 32;
+		sbits = (int)n;
+	}
+	if (prec == DK_C128)
+		k_marginals<double><<<blocks, threads, 0, st>>>((const double2 *)d,
+							       (int)n, sbits, s.partials);
+	else
+		k_marginals<float><<<blocks, threads, 0, st>>>((const float2 *)d,
+							      (int)n, sbits, s.partials);
+	k_marg_finalize<<<1, 64, 0, st>>>(s.partials, blocks, (int)n, s.marg);
+	g_launches += 2;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_measure_collapse(int prec, const void *in, void *out,
+				    unsigned n, unsigned q, double roll,
+				    int forced, const dk_scal *sc_in,
+				    dk_scal *sc_out, const Scratch &s,
+				    cudaStream_t st)
+{
+	k_decide<<<1, 1, 0, st>>>(s.marg, (int)q, roll, forced, sc_in, sc_out);
+	const uint64_t half = 1ull << (n - 1);
+	if (out != nullptr) {
+		const int blocks = grid_for(half, 256 * 4, g_num_sms * 8);
+		if (prec == DK_C128)
+			k_collapse<double><<<blocks, 256, 0, st>>>(
+				(const double2 *)in, (double2 *)out, half, (int)q,
+				sc_out, s.partials);
+		else
+			k_collapse<float><<<blocks, 256, 0, st>>>(
+				(const float2 *)in, (float2 *)out, half, (int)q,
+				sc_out, s.partials);
+		k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc_in, sc_out,
+					       FIN_COLLAPSE, 1);
+	}
+	g_launches += (out != nullptr) ? 3 : 1;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_join(int prec, const void *most, unsigned n1,
+			const dk_scal *sc1, const void *least, unsigned n2,
+			const dk_scal *sc2, void *out, dk_scal *sc_out,
+			const Scratch &s, cudaStream_t st)
+{
+	const uint64_t size = 1ull << (n1 + n2);
+	const int blocks = grid_for(size, 256 * 4, g_num_sms * 8);
+	k_clear_flags<<<1, 1, 0, st>>>(sc_out);
+	if (prec == DK_C128)
+		k_join<double><<<blocks, 256, 0, st>>>((const double2 *)most, sc1,
+						      (const double2 *)least, sc2,
+						      (int)n2, (double2 *)out, size,
+						      s.partials);
+	else
+		k_join<float><<<blocks, 256, 0, st>>>((const float2 *)most, sc1,
+						     (const float2 *)least, sc2, (int)n2,
+						     (float2 *)out, size, s.partials);
+	k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc_out, sc_out, FIN_RESET, 1);
+	g_launches += 3;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_first_nonzero(int prec, const void *d, uint64_t first,
+				 uint64_t count, const Scratch &s, cudaStream_t st)
+{
+	cudaError_t e = cudaMemsetAsync(s.u64, 0xff, sizeof(unsigned long long), st);
+	if (e != cudaSuccess)
+		return e;
+	const int blocks = grid_for(count, 256, g_num_sms * 8);
+	if (prec == DK_C128)
+		k_first_nz<double><<<blocks, 256, 0, st>>>((const double2 *)d, first,
+							  count, s.u64);
+	else
+		k_first_nz<float><<<blocks, 256, 0, st>>>((const float2 *)d, first,
+							 count, s.u64);
+	g_launches += 1;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_gather_kept(int prec, const void *d, unsigned n,
+			       uint64_t keep_mask, double2 *M, cudaStream_t st)
+{
+	const uint64_t full = (n >= 64) ? ~0ull : ((1ull << n) - 1ull);
+	const uint64_t trace = full & ~keep_mask;
+	const int k = __builtin_popcountll(keep_mask);
+	const uint64_t total = 1ull << n;
+	const int blocks = grid_for(total, 256 * 4, g_num_sms * 8);
+	if (prec == DK_C128)
+		k_gather_kept<double><<<blocks, 256, 0, st>>>((const double2 *)d,
+							     keep_mask, trace, k,
+							     total, M);
+	else
+		k_gather_kept<float><<<blocks, 256, 0, st>>>((const float2 *)d,
+							    keep_mask, trace, k, total,
+							    M);
+	g_launches += 1;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_herm_fill(const double2 *C, double2 *rho, uint64_t dim,
+			     cudaStream_t st)
+{
+	const int blocks = grid_for(dim * dim, 256 * 4, g_num_sms * 8);
+	k_herm_fill<<<blocks, 256, 0, st>>>(C, rho, dim);
+	g_launches += 1;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_rho_elem(int prec, const void *d, unsigned n,
+			    uint64_t keep_mask, uint64_t i, uint64_t j,
+			    const dk_scal *sc, const Scratch &s, cudaStream_t st)
+{
+	const uint64_t full = (n >= 64) ? ~0ull : ((1ull << n) - 1ull);
+	const uint64_t trace = full & ~keep_mask;
+	const int t = __builtin_popcountll(trace);
+	/* host-side deposit of the kept indices */
+	uint64_t ia = 0, ib = 0, m = keep_mask;
+	for (uint64_t bit = 1; m; bit <<= 1) {
+		const uint64_t low = m & (~m + 1ull);
+		if (i & bit)
+			ia |= low;
+		if (j & bit)
+			ib |= low;
+		m &= m - 1ull;
+	}
+	const uint64_t cnt = 1ull << t;
+	const int blocks = grid_for(cnt, 256 * 4, g_num_sms * 8);
+	if (prec == DK_C128)
+		k_rho_elem<double><<<blocks, 256, 0, st>>>((const double2 *)d, ia, ib,
+							  trace, cnt, s.partials);
+	else
+		k_rho_elem<float><<<blocks, 256, 0, st>>>((const float2 *)d, ia, ib,
+							 trace, cnt, s.partials);
+	k_rho_elem_finalize<<<1, 32, 0, st>>>(s.partials, blocks, sc, s.marg);
+	g_launches += 2;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_export(int prec, const void *d, uint64_t first, uint64_t count,
+			  double2 *dst, cudaStream_t st)
+{
+	const int blocks = grid_for(count, 256 * 4, g_num_sms * 8);
+	if (prec == DK_C128)
+		k_export<double><<<blocks, 256, 0, st>>>((const double2 *)d, first,
+							count, dst);
+	else
+		k_export<float><<<blocks, 256, 0, st>>>((const float2 *)d, first, count,
+						       dst);
+	g_launches += 1;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_copy(int prec, const void *src, void *dst, unsigned n,
+			const dk_scal *sc_in, dk_scal *sc_out, cudaStream_t st)
+{
+	const size_t bytes = (prec == DK_C128 ? 16 : 8) * ((size_t)1 << n);
+	cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st);
+	if (e != cudaSuccess)
+		return e;
+	k_copy_scal<<<1, 1, 0, st>>>(sc_in, sc_out);
+	g_launches += 1;
+	return cudaGetLastError();
+}
+
+} // namespace dk

@@ -1,0 +1,97 @@
+/* Launch wrappers of the engine's CUDA kernels (internal, C++). */
+#ifndef DK_KERNELS_H_
+#define DK_KERNELS_H_
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dk_internal.h"
+
+namespace dk {
+
+/* Kernels launched by the wrappers below (for the engine's counters). */
+extern unsigned long long g_launches;
+
+/* Number of per-block partial slots the scratch buffer must hold. */
+constexpr int kMaxBlocks = 4096;
+/* doubles per partial slot (marginals need n + 1 <= 64) */
+constexpr int kPartialStride = 64;
+
+struct Scratch {
+	double *partials; /* kMaxBlocks * kPartialStride doubles */
+	unsigned long long *u64; /* 4 words */
+	double *marg; /* 64 doubles: marginal sums + total */
+};
+
+/* fused sweep: in may equal out (in place) */
+cudaError_t launch_sweep(int prec, const void *in, void *out,
+			 const unsigned char *dprog, const dk_sweep_hdr *hprog,
+			 const dk_scal *sc_in, dk_scal *sc_out,
+			 const Scratch &s, int num_sms, cudaStream_t st);
+
+/* generic k-qubit gate, out of place */
+cudaError_t launch_generic_gate(int prec, const void *in, void *out,
+				unsigned n, unsigned k, const unsigned *tg,
+				uint64_t cm, uint64_t am, const double *dmat,
+				const dk_scal *sc_in, dk_scal *sc_out,
+				const Scratch &s, cudaStream_t st);
+
+/* |0..0>: zero + amp[0] = 1, norm = csq = 1 */
+cudaError_t launch_init_zero(int prec, void *d, unsigned n, dk_scal *sc,
+			     cudaStream_t st);
+
+/* convert host-staged complex128 into the buffer's precision (d may alias
+ * src for complex128) and set norm = 1, csq = sum |x|^2 */
+cudaError_t launch_import(int prec, const double *src, void *d, unsigned n,
+			  dk_scal *sc, const Scratch &s, cudaStream_t st);
+
+/* all marginal sums S_q (q < n) and the total into s.marg[0..n] */
+cudaError_t launch_marginals(int prec, const void *d, unsigned n,
+			     const Scratch &s, cudaStream_t st);
+
+/* decide outcome of qubit q against roll (uses s.marg), then gather the
+ * selected half into out (n-1 qubits) */
+cudaError_t launch_measure_collapse(int prec, const void *in, void *out,
+				    unsigned n, unsigned q, double roll,
+				    int forced, const dk_scal *sc_in,
+				    dk_scal *sc_out, const Scratch &s,
+				    cudaStream_t st);
+
+/* out = (most / n1) (x) (least / n2), norm 1 */
+cudaError_t launch_join(int prec, const void *most, unsigned n1,
+			const dk_scal *sc1, const void *least, unsigned n2,
+			const dk_scal *sc2, void *out, dk_scal *sc_out,
+			const Scratch &s, cudaStream_t st);
+
+/* smallest index in [first, first+count) with a non-zero amplitude, or
+ * UINT64_MAX, into s.u64[0] */
+cudaError_t launch_first_nonzero(int prec, const void *d, uint64_t first,
+				 uint64_t count, const Scratch &s,
+				 cudaStream_t st);
+
+/* gather psi into a complex128 matrix M[b][a] (a = kept bits, b = traced) */
+cudaError_t launch_gather_kept(int prec, const void *d, unsigned n,
+			       uint64_t keep_mask, double2 *M, cudaStream_t st);
+
+/* lower triangle of the column-major Hermitian C -> full row-major rho */
+cudaError_t launch_herm_fill(const double2 *C, double2 *rho, uint64_t dim,
+			     cudaStream_t st);
+
+/* one reduced-density element, summed into s.marg[0..1] */
+cudaError_t launch_rho_elem(int prec, const void *d, unsigned n,
+			    uint64_t keep_mask, uint64_t i, uint64_t j,
+			    const dk_scal *sc, const Scratch &s,
+			    cudaStream_t st);
+
+/* copy amplitudes [first, first+count) to complex128 dst (device) */
+cudaError_t launch_export(int prec, const void *d, uint64_t first,
+			  uint64_t count, double2 *dst, cudaStream_t st);
+
+/* D2D copy of a register (clone that must diverge), scalars included */
+cudaError_t launch_copy(int prec, const void *src, void *dst, unsigned n,
+			const dk_scal *sc_in, dk_scal *sc_out,
+			cudaStream_t st);
+
+} // namespace dk
+
+#endif

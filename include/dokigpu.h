@@ -1,0 +1,164 @@
+/*
+ * dokigpu.h -- C ABI of the B200 state-vector engine behind the `doki` module.
+ *
+ * The entry points replace the reference engine's internal C layer (Mowstyl/Doki
+ * src/doki/qstate.h, qops.h, funmatrix.h), which its CPython binding
+ * (src/doki/doki.c) calls; each declaration cites the function it stands in
+ * for.  Plain C types only: opaque handles, pointers, sizes, int status codes.
+ * No call aborts; every failure is a non-zero status (see dk_strerror).
+ *
+ * Layout: a register of n qubits is 2^n amplitudes resident in device memory
+ * (complex128 or complex64, interleaved re/im) plus a device-side FP64
+ * normalisation constant; logical amplitude i = amp[i] / norm, exactly as the
+ * reference's lazy norm (qstate.h:84-86).  Qubit q is bit q of the index.
+ * Host buffers passed to or returned from this ABI are complex128 interleaved
+ * (double re, double im) regardless of the register's storage precision.
+ *
+ * Registers are immutable values with copy-on-write storage: operations that
+ * "return a new register" (apply, clone, measure) share device storage until
+ * one of the sharers needs to diverge, so `r = apply(r, g)` chains run in place
+ * once the previous handle is freed.  Gates queued on a register are fused
+ * into multi-gate sweeps when the register is next read.
+ */
+#ifndef DOKIGPU_H_
+#define DOKIGPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define DK_OK 0
+#define DK_ERR_ALLOC 1 /* allocation failed: state_init codes 1/2, qstate.c:23-88 */
+#define DK_ERR_QUBITS 3 /* too many qubits: state_init code 3, qstate.c:30-32 */
+#define DK_ERR_ARG 20 /* invalid argument (range, overlap, size) */
+#define DK_ERR_CUDA 21 /* a CUDA runtime call failed */
+#define DK_ERR_BUDGET 22 /* the device-memory budget would be exceeded */
+#define DK_ERR_TIMEOUT 23 /* a bounded device wait ran out */
+#define DK_ERR_DEAD 24 /* handle was explicitly freed (registry_del) */
+#define DK_ERR_EMPTY 25 /* operation on a 0-qubit register */
+#define DK_ERR_NORM0 26 /* collapse produced a zero normalisation constant */
+#define DK_ERR_NODEV 27 /* no usable CUDA device */
+
+/* ---- precisions (reference platform.h:199 PRECISION 1 / 2) ------------ */
+#define DK_C64 1 /* complex64 amplitudes, FP64 norm / reductions */
+#define DK_C128 2 /* complex128 amplitudes (the reference's type) */
+
+/* Largest register the engine accepts (the reference's MAX_NUM_QUBITS is 62,
+ * platform.h:270; 2^40 amplitudes already exceed any single device). */
+#define DK_MAX_QUBITS 40
+
+typedef struct dk_state dk_state;
+typedef struct dk_gate dk_gate;
+
+const char *dk_strerror(int status);
+/* Text of the last CUDA error seen by this library (or ""). */
+const char *dk_last_cuda_error(void);
+
+/* Select / initialise the device for this process (default: device 0 on
+ * first use).  Idempotent. */
+int dk_init(int device);
+
+/* ---- gates: struct qgate, qgate.h:25-32; gate_new doki.c:417-512 ---------
+ * matrix: 2^k x 2^k row-major, complex128 interleaved.  Row index bit m is
+ * the value of targets[m] (targets[0] least significant), qops.c:227-240. */
+int dk_gate_new(unsigned num_qubits, const double *matrix, dk_gate **out);
+/* gate_get doki.c:514-544: copy the matrix back (2 * 4^k doubles). */
+int dk_gate_get(const dk_gate *gate, double *matrix);
+unsigned dk_gate_num_qubits(const dk_gate *gate);
+void dk_gate_free(dk_gate *gate);
+
+/* ---- registers: struct state_vector, qstate.h:44-59 --------------------- */
+/* state_init(init=1) qstate.c:23-88 via registry_new doki.c:302-341: |0..0>. */
+int dk_state_new(unsigned num_qubits, int precision, dk_state **out);
+/* registry_new_data doki.c:625-720: 2^n complex128 values from host memory,
+ * stored as given (no normalisation; norm = 1). */
+int dk_state_from_host(unsigned num_qubits, int precision,
+		       const double *values, dk_state **out);
+/* state_clone qstate.c:90-105 (copy-on-write: no device copy is made). */
+int dk_state_clone(dk_state *src, dk_state **out);
+/* registry_del doki.c:400-415: release device storage now; later use of the
+ * handle returns DK_ERR_DEAD.  The handle itself stays valid until freed. */
+void dk_state_release(dk_state *s);
+/* state_clear qstate.c:107-121 + free: drop the handle. */
+void dk_state_free(dk_state *s);
+/* state_mem_size qstate.c:123-135: bytes of device + host storage. */
+size_t dk_state_mem_size(const dk_state *s);
+unsigned dk_state_num_qubits(const dk_state *s);
+int dk_state_precision(const dk_state *s);
+
+/* ---- the hot path: qops.h:28-56 ----------------------------------------- */
+/* apply_gate qops.c:176-261: returns a new register G(controls) * in,
+ * renormalised.  Targets, controls and anticontrols must be distinct and
+ * < num_qubits. */
+int dk_apply_gate(dk_state *in, const dk_gate *gate, const unsigned *targets,
+		  unsigned num_targets, const unsigned *controls,
+		  unsigned num_controls, const unsigned *anticontrols,
+		  unsigned num_anticontrols, dk_state **out);
+
+/* state_get qstate.h:86 (registry_get doki.c:546-595): logical amplitude. */
+int dk_get_amplitude(dk_state *s, uint64_t id, double *re, double *im);
+/* Bulk form of the above: amplitudes [first, first + count) into `out`
+ * (2 * count doubles). */
+int dk_get_amplitudes(dk_state *s, uint64_t first, uint64_t count,
+		      double *out);
+/* get_global_phase qops.c:46-70: arg of the first non-zero amplitude if its
+ * imaginary part is non-zero, else 0 (cached per register). */
+int dk_global_phase(dk_state *s, double *phase);
+
+/* probability qops.c:72-95: P(target = 1). */
+int dk_probability(dk_state *s, unsigned target, double *p);
+/* All n single-qubit marginals P(q = 1) in one sweep (p: n doubles). */
+int dk_marginals(dk_state *s, double *p);
+
+/* measure qops.c:124-136: result = P(target=1) > roll, then collapse
+ * (qops.c:138-174) into a register one qubit smaller (*out = NULL when the
+ * input had one qubit). */
+int dk_measure(dk_state *s, unsigned target, double roll, int *result,
+	       dk_state **out);
+/* registry_measure doki.c:1023-1192: qubits num_qubits-1 .. 0 that are set in
+ * `mask`, one roll each in that order (rolls must be in [0, 1)).  results:
+ * num_qubits entries, results[i] for qubit num_qubits-1-i: -1 = not
+ * measured, 0 / 1 = outcome.  *out = NULL when every qubit was measured. */
+int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
+		    unsigned num_rolls, int8_t *results, dk_state **out);
+
+/* join qops.c:97-122: tensor product, `most` on the high qubits. */
+int dk_join(dk_state *most, dk_state *least, dk_state **out);
+
+/* density_matrix qops.c:580-601 followed by partial_trace funmatrix.c:999-1037
+ * over every qubit outside keep_mask, materialised: out[a * 2^k + a'] =
+ * sum_b psi[a|b] conj(psi[a'|b]) with the k kept qubits, in increasing order,
+ * forming the bits of a.  out: 2 * 4^k doubles, k <= 14. */
+int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out);
+/* One element of the same matrix, for kept sets too large to materialise. */
+int dk_reduced_density_elem(dk_state *s, uint64_t keep_mask, uint64_t i,
+			    uint64_t j, double *re, double *im);
+
+/* Wait for all queued device work of this library. */
+int dk_sync(void);
+
+/* ---- engine controls (no counterpart in the reference) ------------------ */
+/* 1 (default): queued gates are fused into multi-gate sweeps when a register
+ * is read; 0: every gate is its own sweep (the per-gate plain method). */
+int dk_set_fusion(int enable);
+/* Counters since dk_init: CUDA kernels launched by this library, fused
+ * sweeps executed and gates applied by them.  Any pointer may be NULL. */
+int dk_get_stats(uint64_t *kernel_launches, uint64_t *sweeps,
+		 uint64_t *gates_applied);
+/* Bytes copied host->device and device->host by this library since dk_init. */
+int dk_get_io_stats(uint64_t *h2d_bytes, uint64_t *d2h_bytes);
+/* Execute the gates queued on `s` now (normally deferred to the next read). */
+int dk_state_flush(dk_state *s);
+/* The CUDA stream (cudaStream_t) all of this library's work is queued on,
+ * for callers that time it with events; NULL before initialisation. */
+void *dk_stream(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DOKIGPU_H_ */

@@ -1,0 +1,347 @@
+"""Parity of the CUDA engine with the reference: golden fixtures generated from
+the reference module, and the CPU oracle on seeded workloads.
+
+complex128: amplitudes and probabilities within 1e-12 absolute, measurement
+outcomes identical.  complex64: within ATOL_C64 of the complex128 oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from doki_b200 import workloads as W
+from tests.conftest import ATOL_C128, ATOL_C64
+from tests.golden.gen_golden import random_unitary
+from tests.test_plan import random_ops
+
+pytestmark = pytest.mark.gpu
+
+
+def allamps(d, reg, canonical=False):
+    return d.registry_get_all(reg, canonical)
+
+
+def res_list(res):
+    return [-1 if v is None else int(v) for v in res]
+
+
+# ---------------------------------------------------------------- golden ----
+
+def test_golden_small12(dk_gpu, golden):
+    d = dk_gpu
+    c = W.small_circuit(seed=1, n=12, depth=20)
+    reg = W.run_ops(d, d.registry_new(12, False), c.ops)
+    amps = allamps(d, reg)
+    assert np.allclose(amps, golden["small12_amps"], atol=ATOL_C128, rtol=0)
+    # the element-wise reference accessor agrees with the bulk one
+    for i in (0, 1, 777, 4095):
+        assert abs(d.registry_get(reg, i, False, False) - golden["small12_amps"][i]) < ATOL_C128
+    probs = [d.registry_prob(reg, q, 1, False) for q in range(12)]
+    assert np.allclose(probs, golden["small12_probs"], atol=ATOL_C128, rtol=0)
+    r0, res = d.registry_measure(reg, (1 << 12) - 1, golden["small12_rolls"].tolist(), 1, False)
+    assert r0 is None
+    assert res_list(res) == golden["small12_measure_all"].tolist()
+    mask = int(golden["small12_half_mask"][0])
+    r2, res2 = d.registry_measure(reg, mask, golden["small12_half_rolls"].tolist(), 1, False)
+    assert res_list(res2) == golden["small12_half_res"].tolist()
+    assert np.allclose(allamps(d, r2, True), golden["small12_half_amps"], atol=ATOL_C128, rtol=0)
+    # the measured register is untouched
+    assert np.allclose(allamps(d, reg), golden["small12_amps"], atol=ATOL_C128, rtol=0)
+
+
+@pytest.mark.parametrize("n", range(1, 7))
+def test_golden_one_gate(dk_gpu, golden, n):
+    d = dk_gpu
+    reg = d.registry_new(n, False)
+    for q, a in enumerate(golden[f"one_{n}_angles"]):
+        reg = d.registry_apply(reg, d.gate_new(1, W.u3(*a).tolist(), False), [q], None, None,
+                               1, False)
+    assert np.allclose(allamps(d, reg), golden[f"one_{n}_amps"], atol=ATOL_C128, rtol=0)
+
+
+def test_golden_controls(dk_gpu, golden):
+    d = dk_gpu
+    order = golden["ctrl_order"].tolist()
+    g = d.gate_new(1, W.u3(*golden["ctrl_angles"]).tolist(), False)
+    reg = d.registry_apply(d.registry_new(7, False), g, [order[0]], None, None, 1, False)
+    ctl, act, is_c = [], [], True
+    for prev, q in zip(order, order[1:]):
+        (ctl if is_c else act).append(prev)
+        reg = d.registry_apply(reg, g, [q], set(ctl), set(act), 1, False)
+        is_c = not is_c
+    assert np.allclose(allamps(d, reg), golden["ctrl_amps"], atol=ATOL_C128, rtol=0)
+
+
+def test_golden_pairs(dk_gpu, golden):
+    d = dk_gpu
+    base = [W.Op(m, [q]) for q, m in enumerate(golden["pair_base"])]
+    start = W.run_ops(d, d.registry_new(5, False), base)
+    g = d.gate_new(2, golden["pair_u"].tolist(), False)
+    i = 0
+    for a in range(5):
+        for b in range(5):
+            if a != b:
+                r = d.registry_apply(start, g, [a, b], None, None, 1, False)
+                assert np.allclose(allamps(d, r), golden["pair_amps"][i], atol=ATOL_C128,
+                                   rtol=0), (a, b)
+                i += 1
+
+
+def test_golden_three_qubit_and_diagonal(dk_gpu, golden):
+    d = dk_gpu
+    rng = W.rng_for(14)
+    random_unitary(rng, 3)
+    rng.random(4)
+    reg = W.run_ops(d, d.registry_new(6, False),
+                    [W.Op(W.u3(*(rng.random(3) * 2 * np.pi)), [q]) for q in range(6)])
+    u3q, diag2 = golden["k3_u"], golden["k3_diag2"]
+    seq = [(u3q, [4, 0, 2], set(), set()), (diag2, [1, 5], {3}, set()),
+           (u3q, [5, 3, 1], set(), {0}), (u3q, [0, 1, 2], {5}, {4})]
+    for m, tg, cs, acs in seq:
+        reg = d.registry_apply(reg, d.gate_new(len(tg), m.tolist(), False), tg,
+                               cs if (cs or acs) else None, acs or None, 1, False)
+    assert np.allclose(allamps(d, reg), golden["k3_amps"], atol=ATOL_C128, rtol=0)
+
+
+def test_golden_join(dk_gpu, golden):
+    d = dk_gpu
+    regs = [d.registry_apply(d.registry_new(1, False), d.gate_new(1, m.tolist(), False), [0],
+                             None, None, 1, False) for m in golden["join_gates"]]
+    res = regs[0]
+    for r in regs[1:]:
+        res = d.registry_join(res, r, 1, False)
+    assert np.allclose(allamps(d, res), golden["join_amps"], atol=ATOL_C128, rtol=0)
+
+
+def test_golden_density_and_partial_trace(dk_gpu, golden):
+    d = dk_gpu
+    c8 = W.small_circuit(seed=16, n=8, depth=6)
+    reg = W.run_ops(d, d.registry_new(8, False), c8.ops)
+    rho = d.registry_density(reg, False)
+    assert d.funmatrix_shape(rho, False) == (256, 256)
+    diag = [d.funmatrix_get(rho, i, i, False) for i in range(256)]
+    assert np.allclose(diag, golden["rho8_diag"], atol=ATOL_C128, rtol=0)
+    row = [d.funmatrix_get(rho, 5, j, False) for j in range(256)]
+    assert np.allclose(row, golden["rho8_row5"], atol=ATOL_C128, rtol=0)
+    pt = rho
+    for e in golden["rho8_elems"].tolist():
+        pt = d.funmatrix_partialtrace(pt, e, False)
+    assert d.funmatrix_shape(pt, False) == (32, 32)
+    m = np.array([[d.funmatrix_get(pt, i, j, False) for j in range(32)] for i in range(32)])
+    assert np.allclose(m, golden["rho8_ptrace"], atol=ATOL_C128, rtol=0)
+    assert np.allclose(d.funmatrix_numpy(pt), golden["rho8_ptrace"], atol=ATOL_C128, rtol=0)
+    assert abs(d.funmatrix_trace(pt, False) - golden["rho8_ptrace_trace"][0]) < ATOL_C128
+    pt2 = rho
+    for _ in range(5):
+        pt2 = d.funmatrix_partialtrace(pt2, 3, False)
+    assert np.allclose(d.funmatrix_numpy(pt2), golden["rho8_low3"], atol=ATOL_C128, rtol=0)
+
+
+def test_golden_canonical(dk_gpu, golden):
+    d = dk_gpu
+    rng = W.rng_for(17)
+    reg = d.registry_new(4, False)
+    for q in range(4):
+        ph = np.exp(1j * np.pi * (rng.random() * 2 - 1)) * W.H
+        reg = d.registry_apply(reg, d.gate_new(1, ph.tolist(), False), [q], None, None, 1, False)
+    assert np.allclose(allamps(d, reg), golden["canon_raw"], atol=ATOL_C128, rtol=0)
+    can = [d.registry_get(reg, i, True, False) for i in range(16)]
+    assert np.allclose(can, golden["canon_amps"], atol=ATOL_C128, rtol=0)
+    r2, res = d.registry_measure(reg, 1, golden["canon_roll"].tolist(), 1, False)
+    assert res_list(res) == golden["canon_meas_res"].tolist()
+    assert np.allclose(allamps(d, r2, True), golden["canon_meas_amps"], atol=ATOL_C128, rtol=0)
+
+
+def test_golden_unnormalised_data(dk_gpu, golden):
+    d = dk_gpu
+    reg = d.registry_new_data(3, golden["data_vals"], False)
+    assert np.array_equal(allamps(d, reg), golden["data_raw"])
+    assert np.array_equal([d.registry_get(reg, i, False, False) for i in range(8)],
+                          golden["data_raw"])
+    reg_l = d.registry_new_data(3, golden["data_vals"].tolist(), False)
+    assert np.array_equal(allamps(d, reg_l), golden["data_raw"])
+    r2 = d.registry_apply(reg, d.gate_new(1, W.H.tolist(), False), [1], None, None, 1, False)
+    assert np.allclose(allamps(d, r2), golden["data_after_h"], atol=ATOL_C128, rtol=0)
+    probs = [d.registry_prob(reg, q, 1, False) for q in range(3)]
+    assert np.allclose(probs, golden["data_prob"], atol=ATOL_C128, rtol=0)
+
+
+# ---------------------------------------------------------------- oracle ----
+
+@pytest.mark.parametrize("n,count", [(3, 40), (5, 80), (9, 120), (12, 150), (14, 150),
+                                     (16, 120), (19, 60)])
+def test_random_circuits_vs_oracle(dk_gpu, orc, n, count):
+    d = dk_gpu
+    rng = W.rng_for(5000 + n)
+    ops = random_ops(rng, n, count)
+    if n >= 5:
+        ops.insert(count // 2, W.Op(random_unitary(rng, 4), [0, n - 1, 1, n // 2]))
+    a = W.run_ops(d, d.registry_new(n, False), ops)
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    assert np.allclose(allamps(d, a), orc.registry_get_all(b), atol=ATOL_C128, rtol=0)
+    assert np.allclose(d.registry_probs(a), orc.registry_probs(b), atol=ATOL_C128, rtol=0)
+
+
+@pytest.mark.parametrize("fuse", [False, True])
+def test_fused_equals_unfused(dk_gpu, orc, fuse):
+    d = dk_gpu
+    n = 15
+    ops = random_ops(W.rng_for(77), n, 100)
+    d.engine_set_fusion(fuse)
+    try:
+        a = W.run_ops(d, d.registry_new(n, False), ops)
+        got = allamps(d, a)
+    finally:
+        d.engine_set_fusion(True)
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    assert np.allclose(got, orc.registry_get_all(b), atol=ATOL_C128, rtol=0)
+
+
+def test_copy_on_write_semantics(dk_gpu):
+    """Every operation returns a new register; inputs are never mutated."""
+    d = dk_gpu
+    n = 14
+    g = d.gate_new(1, W.H.tolist(), False)
+    r0 = d.registry_new(n, False)
+    r1 = d.registry_apply(r0, g, [0], None, None, 1, False)
+    r2 = d.registry_apply(r1, g, [13], None, None, 1, False)
+    c2 = d.registry_clone(r2, 1, False)
+    r3 = d.registry_apply(r2, g, [0], None, None, 1, False)
+    v0, v1, v2, v3 = (allamps(d, r) for r in (r0, r1, r2, r3))
+    assert v0[0] == 1 and np.count_nonzero(v0) == 1
+    assert np.allclose(abs(v1[[0, 1]]), 2 ** -0.5) and np.count_nonzero(np.abs(v1) > 1e-15) == 2
+    assert np.count_nonzero(np.abs(v2) > 1e-15) == 4
+    assert np.allclose(abs(v3[[0, 1 << 13]]), 2 ** -0.5)
+    assert np.allclose(allamps(d, c2), v2, atol=0)
+    d.registry_del(r1, False)
+    with pytest.raises(d.error):
+        d.registry_get(r1, 0, False, False)
+    assert np.allclose(allamps(d, r2), v2, atol=0)
+
+
+def test_measure_sequence_vs_oracle(dk_gpu, orc):
+    d = dk_gpu
+    n = 16
+    ops = random_ops(W.rng_for(31), n, 120)
+    a = W.run_ops(d, d.registry_new(n, False), ops)
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    rng = W.rng_for(32)
+    for trial in range(6):
+        mask = int(rng.integers(1, 1 << n))
+        rolls = rng.random(bin(mask).count("1")).tolist()
+        ra, resa = d.registry_measure(a, mask, rolls, 1, False)
+        rb, resb = orc.registry_measure(b, mask, rolls)
+        assert res_list(resa) == res_list(resb), trial
+        if rb is not None:
+            assert np.allclose(allamps(d, ra), orc.registry_get_all(rb), atol=ATOL_C128, rtol=0)
+
+
+def test_reduced_density_vs_oracle(dk_gpu, orc, oracle_mod):
+    d = dk_gpu
+    n = 14
+    ops = random_ops(W.rng_for(41), n, 100)
+    a = W.run_ops(d, d.registry_new(n, False), ops)
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    rho = d.registry_density(a, False)
+    # keep the low 6 qubits (trace out 13..6)
+    pt = rho
+    for e in range(n - 1, 5, -1):
+        pt = d.funmatrix_partialtrace(pt, e, False)
+    want = oracle_mod.reduced_density(b, 0b111111)
+    assert np.allclose(d.funmatrix_numpy(pt), want, atol=ATOL_C128, rtol=0)
+    # a scattered kept set
+    elems = [12, 9, 9, 4, 0, 3, 1]
+    pt = rho
+    for e in elems:
+        pt = d.funmatrix_partialtrace(pt, e, False)
+    keep = oracle_mod.kept_mask_after_traces(n, elems)
+    want = oracle_mod.reduced_density(b, keep)
+    got = d.funmatrix_numpy(pt)
+    assert np.allclose(got, want, atol=ATOL_C128, rtol=0)
+    assert abs(d.funmatrix_trace(pt, False) - np.trace(want)) < 1e-11
+
+
+def test_join_vs_oracle(dk_gpu, orc):
+    d = dk_gpu
+    oa = random_ops(W.rng_for(51), 9, 60)
+    ob = random_ops(W.rng_for(52), 8, 60)
+    a = W.run_ops(d, d.registry_new(9, False), oa)
+    b = W.run_ops(d, d.registry_new(8, False), ob)
+    j = d.registry_join(a, b, 1, False)
+    ja = W.run_ops(orc, orc.registry_new(9), oa)
+    jb = W.run_ops(orc, orc.registry_new(8), ob)
+    jo = orc.registry_join(ja, jb)
+    assert np.allclose(allamps(d, j), orc.registry_get_all(jo), atol=ATOL_C128, rtol=0)
+
+
+def test_canonical_phase_vs_oracle(dk_gpu, orc):
+    d = dk_gpu
+    n = 12
+    ops = random_ops(W.rng_for(61), n, 50)
+    # zero out a leading block so the first non-zero amplitude is not index 0
+    ops.append(W.Op(np.array([[0, 0], [0, 1]], dtype=complex), [0]))
+    ops.append(W.Op(np.array([[0, 0], [0, 1]], dtype=complex), [3]))
+    a = W.run_ops(d, d.registry_new(n, False), ops)
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    assert np.allclose(allamps(d, a, True), orc.registry_get_all(b, canonical=True),
+                       atol=ATOL_C128, rtol=0)
+
+
+def test_inverse_circuit_roundtrip_24q(dk_gpu):
+    """Size-independent property at 24 qubits: U then U^dagger returns |0>."""
+    d = dk_gpu
+    n = 24
+    ops = random_ops(W.rng_for(71), n, 150)
+    inv = [W.Op(op.gate.conj().T, op.targets, op.controls, op.anticontrols)
+           for op in reversed(ops)]
+    r = W.run_ops(d, d.registry_new(n, False), ops + inv)
+    assert abs(d.registry_get(r, 0, False, False) - 1) < 1e-12
+    p = d.registry_probs(r)
+    assert max(p) < 1e-12
+
+
+def test_complex64_vs_complex128_oracle(dk_gpu, orc):
+    d = dk_gpu
+    n = 16
+    ops = random_ops(W.rng_for(81), n, 150)
+    a = W.run_ops(d, d.registry_new(n, False, 1), ops)
+    assert d.registry_precision(a) == 1
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    va, vb = allamps(d, a), orc.registry_get_all(b)
+    assert np.max(np.abs(va - vb)) < ATOL_C64
+    fid = abs(np.vdot(vb, va)) ** 2 / (np.vdot(va, va).real * np.vdot(vb, vb).real)
+    assert fid > 1 - 1e-6
+    assert np.allclose(d.registry_probs(a), orc.registry_probs(b), atol=ATOL_C64)
+    rolls = [0.3, 0.7, 0.1]
+    ra, resa = d.registry_measure(a, 0b1010000000001, rolls, 1, False)
+    rb, resb = orc.registry_measure(b, 0b1010000000001, rolls)
+    assert res_list(resa) == res_list(resb)
+
+
+# ------------------------------------------------------- error behaviour ----
+
+def test_device_side_errors(dk_gpu):
+    d = dk_gpu
+    r = d.registry_new(3, False)
+    g = d.gate_new(1, W.X.tolist(), False)
+    msgs = {}
+    for name, f in [
+        ("actrl_none", lambda: d.registry_apply(r, g, [0], None, {1}, 1, False)),
+        ("same", lambda: d.registry_apply(r, g, [0], {1}, {1}, 1, False)),
+        ("tinc", lambda: d.registry_apply(r, g, [1], {1}, None, 1, False)),
+        ("oor", lambda: d.registry_apply(r, g, [5], None, None, 1, False)),
+        ("ntg", lambda: d.registry_apply(r, g, [0, 1], None, None, 1, False)),
+        ("roll", lambda: d.registry_measure(r, 1, [1.0], 1, False)),
+        ("short", lambda: d.registry_measure(r, 3, [0.5], 1, False)),
+    ]:
+        with pytest.raises(d.error) as ei:
+            f()
+        msgs[name] = str(ei.value)
+    assert msgs["actrl_none"] == "A control cannot also be an anticontrol"
+    assert msgs["same"] == "A control cannot also be an anticontrol"
+    assert msgs["tinc"] == "A target cannot also be a control or an anticontrol"
+    assert msgs["oor"] == "Target qubit out of range"
+    assert msgs["ntg"] == "Wrong number of targets specified for that gate"
+    assert msgs["roll"] == msgs["short"] == "roll not in interval [0, 1)!"
+    r0, res = d.registry_measure(r, 0, [], 1, False)
+    assert res == [None, None, None] and r0 is not None

@@ -1,0 +1,124 @@
+"""Pin the CPU oracle: restatement vs the golden fixtures generated from the
+reference module, and vs the reference module itself where it is built."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from doki_b200 import workloads as W
+from tests.golden.gen_golden import ops_digest, random_unitary
+
+ATOL = 1e-13
+
+
+def test_generator_is_stable(golden):
+    c = W.small_circuit(seed=1, n=12, depth=20)
+    assert ops_digest(c.ops).encode() == golden["small12_digest"].tobytes()
+    c8 = W.small_circuit(seed=16, n=8, depth=6)
+    assert ops_digest(c8.ops).encode() == golden["rho8_digest"].tobytes()
+
+
+def test_small12_circuit(orc, golden):
+    c = W.small_circuit(seed=1, n=12, depth=20)
+    reg = W.run_ops(orc, orc.registry_new(12), c.ops)
+    assert np.allclose(orc.registry_get_all(reg), golden["small12_amps"], atol=ATOL, rtol=0)
+    assert np.allclose(orc.registry_probs(reg), golden["small12_probs"], atol=ATOL, rtol=0)
+    _, res = orc.registry_measure(reg, (1 << 12) - 1, golden["small12_rolls"].tolist())
+    assert [-1 if v is None else int(v) for v in res] == golden["small12_measure_all"].tolist()
+    mask = int(golden["small12_half_mask"][0])
+    r2, res2 = orc.registry_measure(reg, mask, golden["small12_half_rolls"].tolist())
+    assert [-1 if v is None else int(v) for v in res2] == golden["small12_half_res"].tolist()
+    assert np.allclose(orc.registry_get_all(r2, canonical=True), golden["small12_half_amps"],
+                       atol=ATOL, rtol=0)
+
+
+@pytest.mark.parametrize("n", range(1, 7))
+def test_one_gate(orc, golden, n):
+    reg = orc.registry_new(n)
+    for q, a in enumerate(golden[f"one_{n}_angles"]):
+        reg = orc.registry_apply(reg, orc.gate_new(1, W.u3(*a)), [q], None, None)
+    assert np.allclose(orc.registry_get_all(reg), golden[f"one_{n}_amps"], atol=ATOL, rtol=0)
+
+
+def test_controls(orc, golden):
+    order = golden["ctrl_order"].tolist()
+    g = orc.gate_new(1, W.u3(*golden["ctrl_angles"]))
+    reg = orc.registry_apply(orc.registry_new(7), g, [order[0]], None, None)
+    ctl, act, is_c = [], [], True
+    for prev, q in zip(order, order[1:]):
+        (ctl if is_c else act).append(prev)
+        reg = orc.registry_apply(reg, g, [q], set(ctl), set(act))
+        is_c = not is_c
+    assert np.allclose(orc.registry_get_all(reg), golden["ctrl_amps"], atol=ATOL, rtol=0)
+
+
+def test_pairs(orc, golden):
+    base = [W.Op(m, [q]) for q, m in enumerate(golden["pair_base"])]
+    start = W.run_ops(orc, orc.registry_new(5), base)
+    g = orc.gate_new(2, golden["pair_u"])
+    i = 0
+    for a in range(5):
+        for b in range(5):
+            if a != b:
+                r = orc.registry_apply(start, g, [a, b], None, None)
+                assert np.allclose(orc.registry_get_all(r), golden["pair_amps"][i],
+                                   atol=ATOL, rtol=0)
+                i += 1
+
+
+def test_join(orc, golden):
+    regs = [orc.registry_apply(orc.registry_new(1), orc.gate_new(1, m), [0], None, None)
+            for m in golden["join_gates"]]
+    res = regs[0]
+    for r in regs[1:]:
+        res = orc.registry_join(res, r)
+    assert np.allclose(orc.registry_get_all(res), golden["join_amps"], atol=ATOL, rtol=0)
+
+
+def test_partial_trace(orc, oracle_mod, golden):
+    c8 = W.small_circuit(seed=16, n=8, depth=6)
+    reg = W.run_ops(orc, orc.registry_new(8), c8.ops)
+    rho = orc.registry_density(reg)
+    diag = [orc.funmatrix_get(rho, i, i) for i in range(256)]
+    assert np.allclose(diag, golden["rho8_diag"], atol=ATOL, rtol=0)
+    pt = rho
+    for e in golden["rho8_elems"].tolist():
+        pt = orc.funmatrix_partialtrace(pt, e)
+    m = np.array([[orc.funmatrix_get(pt, i, j) for j in range(32)] for i in range(32)])
+    assert np.allclose(m, golden["rho8_ptrace"], atol=ATOL, rtol=0)
+    keep = oracle_mod.kept_mask_after_traces(8, golden["rho8_elems"].tolist())
+    assert np.allclose(oracle_mod.reduced_density(reg, keep), golden["rho8_ptrace"],
+                       atol=ATOL, rtol=0)
+    assert np.allclose(oracle_mod.reduced_density(reg, 0b111), golden["rho8_low3"],
+                       atol=ATOL, rtol=0)
+
+
+def test_unnormalised_data(orc, golden):
+    reg = orc.registry_new_data(3, golden["data_vals"])
+    assert np.allclose(orc.registry_get_all(reg), golden["data_raw"], atol=0, rtol=0)
+    r2 = orc.registry_apply(reg, orc.gate_new(1, W.H), [1], None, None)
+    assert np.allclose(orc.registry_get_all(r2), golden["data_after_h"], atol=ATOL, rtol=0)
+    assert np.allclose([orc.registry_prob(reg, q) for q in range(3)], golden["data_prob"],
+                       atol=ATOL, rtol=0)
+
+
+def test_oracle_vs_reference_random(orc, ref):
+    """Extra cases straight against the reference module (this container)."""
+    rng = W.rng_for(99)
+    for n in (3, 6, 9):
+        ops = []
+        for _ in range(25):
+            k = int(rng.integers(1, 4)) if n >= 3 else 1
+            tg = [int(x) for x in rng.choice(n, size=k, replace=False)]
+            free = [q for q in range(n) if q not in tg]
+            nc = int(rng.integers(0, min(3, len(free)) + 1))
+            cs = [int(x) for x in rng.choice(free, size=nc, replace=False)] if nc else []
+            ctl = {q for q in cs if rng.random() < 0.5}
+            act = set(cs) - ctl
+            ops.append(W.Op(random_unitary(rng, k), tg, ctl, act))
+        a = W.run_ops(ref, ref.registry_new(n, False), ops)
+        b = W.run_ops(orc, orc.registry_new(n), ops)
+        va = np.array([ref.registry_get(a, i, False, False) for i in range(1 << n)])
+        assert np.allclose(va, orc.registry_get_all(b), atol=ATOL, rtol=0)
+        pa = [ref.registry_prob(a, q, 1, False) for q in range(n)]
+        assert np.allclose(pa, orc.registry_probs(b), atol=ATOL, rtol=0)

@@ -1,0 +1,235 @@
+"""Host logic of the gate-fusion planner (doki_b200/csrc/dk_plan.c), on CPU.
+
+The planner's sweep programs are read back through ctypes and replayed by a
+numpy model of the sweep kernel's semantics (tile gather over the sweep's
+qubit set, passes in order, gates with local / per-tile controls, packed
+matrices).  The replay must equal gate-by-gate application by the oracle.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from doki_b200 import workloads as W
+from tests.conftest import ROOT
+from tests.golden.gen_golden import random_unitary
+
+MAXK = 10
+
+
+class FlatOp(ctypes.Structure):
+    _fields_ = [("gate", ctypes.c_void_p), ("k", ctypes.c_uint),
+                ("tg", ctypes.c_uint * MAXK), ("cm", ctypes.c_uint64),
+                ("am", ctypes.c_uint64)]
+
+
+class Limits(ctypes.Structure):
+    _fields_ = [("tile_bits", ctypes.c_int), ("low_bits", ctypes.c_int),
+                ("max_gates", ctypes.c_int), ("max_passes", ctypes.c_int),
+                ("max_mat", ctypes.c_int), ("fuse", ctypes.c_int)]
+
+
+class Step(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("prog_off", ctypes.c_size_t),
+                ("op_index", ctypes.c_int), ("ngates", ctypes.c_int)]
+
+
+class Plan(ctypes.Structure):
+    _fields_ = [("steps", ctypes.POINTER(Step)), ("nsteps", ctypes.c_int),
+                ("blob", ctypes.POINTER(ctypes.c_ubyte)), ("blob_bytes", ctypes.c_size_t)]
+
+
+HDR = np.dtype([("m", "<i4"), ("n", "<i4"), ("npass", "<i4"), ("ngate", "<i4"),
+                ("all_touched", "<i4"), ("pad", "<i4"), ("ntiles", "<u8"),
+                ("qpos", "u1", 16), ("pass_off", "<u4"), ("gate_off", "<u4"),
+                ("mat_off", "<u4"), ("bytes", "<u4")])
+PASS = np.dtype([("b", "u1", 3), ("nlane", "u1"), ("lane", "u1", 16), ("g0", "<u2"),
+                 ("g1", "<u2"), ("pad", "<u4")])
+GATE = np.dtype([("kind", "u1"), ("k", "u1"), ("t", "u1", 3), ("pad", "u1", 3),
+                 ("lc", "<u4"), ("la", "<u4"), ("gc", "<u8"), ("ga", "<u8"),
+                 ("mat", "<u4"), ("pad3", "<u4")])
+assert HDR.itemsize == 64 and PASS.itemsize == 28 and GATE.itemsize == 40
+
+
+@pytest.fixture(scope="module")
+def lib():
+    L = ctypes.CDLL(os.path.join(ROOT, "doki_b200", "libdokigpu.so"))
+    L.dk_gate_new.argtypes = [ctypes.c_uint, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.dk_plan_default_limits.argtypes = [ctypes.c_int, ctypes.c_uint, ctypes.POINTER(Limits)]
+    L.dk_plan_build.argtypes = [ctypes.POINTER(FlatOp), ctypes.c_int, ctypes.c_uint,
+                                ctypes.c_int, ctypes.POINTER(Limits), ctypes.POINTER(Plan)]
+    L.dk_plan_free.argtypes = [ctypes.POINTER(Plan)]
+    L.dk_gate_free.argtypes = [ctypes.c_void_p]
+    return L
+
+
+def build_plan(lib, ops, n, prec=2, fuse=1, tile_bits=None):
+    gates, flat = [], (FlatOp * len(ops))()
+    for i, op in enumerate(ops):
+        m = np.ascontiguousarray(op.gate, dtype=np.complex128)
+        g = ctypes.c_void_p()
+        assert lib.dk_gate_new(op.k, m.ctypes.data, ctypes.byref(g)) == 0
+        gates.append(g)
+        flat[i].gate = g
+        flat[i].k = op.k
+        for j, t in enumerate(op.targets):
+            flat[i].tg[j] = t
+        flat[i].cm = sum(1 << c for c in op.controls)
+        flat[i].am = sum(1 << c for c in op.anticontrols)
+    lim = Limits()
+    lib.dk_plan_default_limits(prec, n, ctypes.byref(lim))
+    lim.fuse = fuse
+    if tile_bits is not None:
+        lim.tile_bits = tile_bits
+    plan = Plan()
+    assert lib.dk_plan_build(flat, len(ops), n, prec, ctypes.byref(lim), ctypes.byref(plan)) == 0
+    blob = bytes(ctypes.cast(plan.blob, ctypes.POINTER(ctypes.c_ubyte * plan.blob_bytes))
+                 .contents) if plan.blob_bytes else b""
+    steps = [(plan.steps[i].kind, plan.steps[i].prog_off, plan.steps[i].op_index)
+             for i in range(plan.nsteps)]
+    lib.dk_plan_free(ctypes.byref(plan))
+    for g in gates:
+        lib.dk_gate_free(g)
+    return steps, blob
+
+
+def apply_local(vec, mat, tbits, ok):
+    """Apply a 2^k x 2^k matrix on local bits `tbits` (targets[0] = LSB) to the
+    entries of `vec` whose boolean mask `ok` holds."""
+    k = len(tbits)
+    out = vec.copy()
+    idx = np.arange(vec.size)
+    tmask = sum(1 << b for b in tbits)
+    bases = idx[(idx & tmask) == 0]
+    for b in bases:
+        if not ok[b]:
+            continue
+        members = [b | sum(((g >> j) & 1) << tbits[j] for j in range(k)) for g in range(1 << k)]
+        out[members] = mat @ vec[members]
+    return out
+
+
+def replay_sweep(blob, off, psi):
+    h = np.frombuffer(blob, HDR, 1, off)[0]
+    m, n = int(h["m"]), int(h["n"])
+    qpos = [int(x) for x in h["qpos"][:m]]
+    passes = np.frombuffer(blob, PASS, int(h["npass"]), off + int(h["pass_off"]))
+    gates = np.frombuffer(blob, GATE, int(h["ngate"]), off + int(h["gate_off"]))
+    nmat = (int(h["bytes"]) - int(h["mat_off"])) // 16
+    mats = np.frombuffer(blob, np.complex128, nmat, off + int(h["mat_off"]))
+    qmask = sum(1 << q for q in qpos)
+    out = psi.copy()
+    local = np.arange(1 << m)
+    offs = np.zeros(1 << m, dtype=np.int64)
+    for j, q in enumerate(qpos):
+        offs |= ((local >> j) & 1) << q
+    rest = [q for q in range(n) if not (qmask >> q) & 1]
+    for t in range(int(h["ntiles"])):
+        base = sum(((t >> j) & 1) << q for j, q in enumerate(rest))
+        tile = out[base | offs].copy()
+        for p in passes:
+            for gi in range(int(p["g0"]), int(p["g1"])):
+                g = gates[gi]
+                gc, ga = int(g["gc"]), int(g["ga"])
+                if (base & gc) != gc or (base & ga):
+                    continue
+                lc, la = int(g["lc"]), int(g["la"])
+                ok = ((local & lc) == lc) & ((local & la) == 0)
+                k = int(g["k"])
+                tb = [int(p["b"][int(g["t"][j])]) for j in range(k)]
+                kind, mo = int(g["kind"]), int(g["mat"])
+                if kind == 1 or kind == 4 or kind == 5:
+                    mat = mats[mo:mo + (1 << 2 * k)].reshape(1 << k, 1 << k)
+                elif kind == 2:
+                    mat = np.diag(mats[mo:mo + 2])
+                elif kind == 3:
+                    mat = np.array([[0, mats[mo]], [mats[mo + 1], 0]])
+                elif kind == 6:
+                    mat = np.diag(mats[mo:mo + (1 << k)])
+                else:
+                    raise AssertionError(kind)
+                tile = apply_local(tile, mat, tb, ok)
+        out[base | offs] = tile
+    return out
+
+
+def run_plan(lib, ops, n, psi, **kw):
+    steps, blob = build_plan(lib, ops, n, **kw)
+    for kind, off, opi in steps:
+        if kind == 1:
+            psi = replay_sweep(blob, off, psi)
+        else:
+            op = ops[opi]
+            cm = sum(1 << c for c in op.controls)
+            am = sum(1 << c for c in op.anticontrols)
+            idx = np.arange(psi.size)
+            ok = ((idx & cm) == cm) & ((idx & am) == 0)
+            psi = apply_local(psi, op.gate, list(op.targets), ok)
+    return psi, steps
+
+
+def oracle_run(orc, ops, n):
+    reg = W.run_ops(orc, orc.registry_new(n), ops)
+    return orc.registry_get_all(reg) * reg.norm  # raw (unnormalised) product
+
+
+def random_ops(rng, n, count, kmax=3):
+    ops = []
+    for _ in range(count):
+        k = int(rng.integers(1, min(kmax, n) + 1))
+        tg = [int(x) for x in rng.choice(n, size=k, replace=False)]
+        free = [q for q in range(n) if q not in tg]
+        nc = int(rng.integers(0, min(3, len(free)) + 1)) if rng.random() < 0.4 else 0
+        cs = [int(x) for x in rng.choice(free, size=nc, replace=False)] if nc else []
+        ctl = {q for q in cs if rng.random() < 0.5}
+        r = rng.random()
+        if k == 1 and r < 0.2:
+            m = W.X.copy()
+        elif k == 1 and r < 0.4:
+            m = np.diag(np.exp(2j * np.pi * rng.random(2)))
+        elif k == 2 and r < 0.3:
+            m = np.diag(np.exp(2j * np.pi * rng.random(4)))
+        else:
+            m = random_unitary(rng, k)
+        ops.append(W.Op(m, tg, ctl, set(cs) - ctl))
+    return ops
+
+
+@pytest.mark.parametrize("n,tile_bits", [(5, None), (8, None), (10, 6), (11, 7), (12, 8)])
+def test_plan_replay_matches_oracle(lib, orc, n, tile_bits):
+    rng = W.rng_for(1000 + n)
+    ops = random_ops(rng, n, 60)
+    ops.append(W.Op(random_unitary(rng, 4), [0, n - 1, 2, n - 2]))  # generic step
+    ops += random_ops(rng, n, 20)
+    psi0 = np.zeros(1 << n, dtype=np.complex128)
+    psi0[0] = 1
+    got, steps = run_plan(lib, ops, n, psi0, tile_bits=tile_bits)
+    want = oracle_run(orc, ops, n)
+    assert np.allclose(got / np.linalg.norm(got), want / np.linalg.norm(want), atol=1e-12)
+    assert any(s[0] == 2 for s in steps)
+    assert sum(1 for s in steps if s[0] == 1) < len(ops) / 2  # fusion happened
+
+
+def test_plan_unfused_one_gate_per_sweep(lib, orc):
+    n = 9
+    ops = random_ops(W.rng_for(7), n, 30)
+    psi0 = np.zeros(1 << n, dtype=np.complex128)
+    psi0[0] = 1
+    got, steps = run_plan(lib, ops, n, psi0, fuse=0, tile_bits=6)
+    assert len(steps) == len(ops)
+    want = oracle_run(orc, ops, n)
+    assert np.allclose(got / np.linalg.norm(got), want / np.linalg.norm(want), atol=1e-12)
+
+
+def test_plan_scale_circuit_fusion_ratio(lib):
+    """At 30 qubits the depth-40 workload fuses into ~2 sweeps per layer."""
+    c = W.scale_circuit(seed=2, n=30, depth=40)
+    steps, blob = build_plan(lib, c.ops, 30)
+    nsweeps = sum(1 for s in steps if s[0] == 1)
+    assert all(s[0] == 1 for s in steps)
+    assert nsweeps <= 3 * c.depth
+    tot = sum(int(np.frombuffer(blob, HDR, 1, off)[0]["ngate"]) for _, off, _ in steps)
+    assert tot == len(c.ops)

@@ -622,7 +622,8 @@ __global__ void __launch_bounds__(256)
 {
 	const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	const int nb = n - s;
-	const uint64_t cnt = 1ull << nb;
+	/* registers smaller than one warp: lanes past the register stay idle */
+	const uint64_t cnt = (g >> s) ? 0ull : (1ull << nb);
 	double tot = 0.0;
 	double hi[kMargHi];
 #pragma unroll

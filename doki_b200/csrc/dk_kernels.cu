@@ -693,6 +693,7 @@ __global__ void k_decide(const double *marg, int q, double roll, int forced,
 	const int res = forced >= 0 ? forced : (p1 > roll ? 1 : 0);
 	sc_out->flag = res;
 	sc_out->p_sel = res ? p1 : 1.0 - p1;
+	sc_out->zero_norm = 0;
 }
 
 /* qops.c:138-174: out[j] = in[insert bit q = outcome into j] */

@@ -92,6 +92,8 @@ void dev_free(void *p, size_t bytes)
 
 /* ---- buffers ------------------------------------------------------------ */
 
+void buf_release(dk_buf *b);
+
 int buf_new(unsigned n, int prec, dk_buf **out)
 {
 	dk_buf *b = (dk_buf *)calloc(1, sizeof(dk_buf));
@@ -111,6 +113,12 @@ int buf_new(unsigned n, int prec, dk_buf **out)
 		dev_free(b->d, b->bytes);
 		free(b);
 		return rc;
+	}
+	/* pool memory is recycled: start every scalar block from zero */
+	cudaError_t e = cudaMemsetAsync(b->sc, 0, sizeof(dk_scal), g.st);
+	if (e != cudaSuccess) {
+		buf_release(b);
+		return cuda_fail(e);
 	}
 	*out = b;
 	return DK_OK;

@@ -276,6 +276,22 @@ __device__ __forceinline__ void apply_gate(C2 (&a)[8], const uint32_t (&loc)[8],
 __device__ __forceinline__ void block_sum2(double &x, double &y)
 {
 	__shared__ double red[2][32];
+	if (blockDim.x < 32) {
+		/* partial warp (sweeps of registers below 8 qubits): no shuffles */
+		red[0][threadIdx.x] = x;
+		red[1][threadIdx.x] = y;
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			x = 0.0;
+			y = 0.0;
+			for (unsigned i = 0; i < blockDim.x; ++i) {
+				x += red[0][i];
+				y += red[1][i];
+			}
+		}
+		__syncthreads();
+		return;
+	}
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1) {
 		x += __shfl_xor_sync(0xffffffffu, x, o);

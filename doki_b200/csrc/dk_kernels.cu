@@ -372,8 +372,9 @@ __global__ void __launch_bounds__(1 << (M - 3), 1)
 		const int gw = (int)(ngate * sizeof(dk_gate_desc) / 4);
 		for (int i = tid; i < gw; i += blockDim.x)
 			dst[i] = __ldg(src + i);
-		if (tid < 16)
-			sq[tid] = h->qpos[tid];
+		/* blocks can be narrower than 16 threads (registers below 7 qubits) */
+		for (int i = tid; i < 16; i += blockDim.x)
+			sq[i] = h->qpos[i];
 	}
 	__syncthreads();
 	const double2 *mats = reinterpret_cast<const double2 *>(prog + h->mat_off);

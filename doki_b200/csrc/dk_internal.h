@@ -90,6 +90,8 @@ enum {
 	DK_GK_DENSE2 = 4,
 	DK_GK_DENSE3 = 5,
 	DK_GK_DIAGK = 6,
+	DK_GK_SWAP1 = 7, /* [[0,1],[1,0]]: exchange, no arithmetic */
+	DK_GK_PHASE1 = 8, /* diag(1, d): scale the |1> half only */
 };
 
 typedef struct dk_gate_desc {

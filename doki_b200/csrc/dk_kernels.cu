@@ -89,7 +89,7 @@ __device__ __forceinline__ bool ctl_ok(uint32_t loc, uint32_t lc, uint32_t la)
  * a[r] holds the amplitude whose pass bits equal r; loc[r] is its tile
  * index (for local control predicates).  t_m: register bit of gate bit m. */
 
-template <int T, typename C2>
+template <int T, bool CTL, typename C2>
 __device__ __forceinline__ void g_dense1(C2 (&a)[8], const uint32_t (&loc)[8],
 					 uint32_t lc, uint32_t la, const double2 *mt)
 {
@@ -100,7 +100,7 @@ __device__ __forceinline__ void g_dense1(C2 (&a)[8], const uint32_t (&loc)[8],
 		if (r & (1 << T))
 			continue;
 		const int r1 = r | (1 << T);
-		if (ctl_ok(loc[r], lc, la)) {
+		if (!CTL || ctl_ok(loc[r], lc, la)) {
 			const C2 x = a[r], y = a[r1];
 			a[r] = cmad(m01, y, cmul(m00, x));
 			a[r1] = cmad(m11, y, cmul(m10, x));
@@ -124,6 +124,37 @@ __device__ __forceinline__ void g_anti1(C2 (&a)[8], const uint32_t (&loc)[8],
 			a[r1] = cmul(m10, x);
 		}
 	}
+}
+
+/* [[0,1],[1,0]] (X and its controlled forms): a pure exchange */
+template <int T, bool CTL, typename C2>
+__device__ __forceinline__ void g_swap1(C2 (&a)[8], const uint32_t (&loc)[8],
+					uint32_t lc, uint32_t la)
+{
+#pragma unroll
+	for (int r = 0; r < 8; ++r) {
+		if (r & (1 << T))
+			continue;
+		const int r1 = r | (1 << T);
+		if (!CTL || ctl_ok(loc[r], lc, la)) {
+			const C2 x = a[r];
+			a[r] = a[r1];
+			a[r1] = x;
+		}
+	}
+}
+
+/* diag(1, d) (Z, S, T, phase and their controlled forms): scale |1> only */
+template <bool CTL, typename C2>
+__device__ __forceinline__ void g_phase1(C2 (&a)[8], const uint32_t (&loc)[8],
+					 uint32_t lc, uint32_t la, int t,
+					 const double2 *mt)
+{
+	const C2 d1 = ldm<C2>(mt);
+#pragma unroll
+	for (int r = 0; r < 8; ++r)
+		if (((r >> t) & 1) && (!CTL || ctl_ok(loc[r], lc, la)))
+			a[r] = cmul(d1, a[r]);
 }
 
 template <typename C2>
@@ -229,14 +260,47 @@ __device__ __forceinline__ void apply_gate(C2 (&a)[8], const uint32_t (&loc)[8],
 {
 	const double2 *mt = mats + gd.mat;
 	const uint32_t lc = gd.lc, la = gd.la;
+	const bool ctl = (lc | la) != 0;
 	switch (gd.kind) {
 	case DK_GK_DENSE1:
-		if (gd.t0 == 0)
-			g_dense1<0>(a, loc, lc, la, mt);
-		else if (gd.t0 == 1)
-			g_dense1<1>(a, loc, lc, la, mt);
+		if (ctl) {
+			if (gd.t0 == 0)
+				g_dense1<0, true>(a, loc, lc, la, mt);
+			else if (gd.t0 == 1)
+				g_dense1<1, true>(a, loc, lc, la, mt);
+			else
+				g_dense1<2, true>(a, loc, lc, la, mt);
+		} else {
+			if (gd.t0 == 0)
+				g_dense1<0, false>(a, loc, lc, la, mt);
+			else if (gd.t0 == 1)
+				g_dense1<1, false>(a, loc, lc, la, mt);
+			else
+				g_dense1<2, false>(a, loc, lc, la, mt);
+		}
+		break;
+	case DK_GK_SWAP1:
+		if (ctl) {
+			if (gd.t0 == 0)
+				g_swap1<0, true>(a, loc, lc, la);
+			else if (gd.t0 == 1)
+				g_swap1<1, true>(a, loc, lc, la);
+			else
+				g_swap1<2, true>(a, loc, lc, la);
+		} else {
+			if (gd.t0 == 0)
+				g_swap1<0, false>(a, loc, lc, la);
+			else if (gd.t0 == 1)
+				g_swap1<1, false>(a, loc, lc, la);
+			else
+				g_swap1<2, false>(a, loc, lc, la);
+		}
+		break;
+	case DK_GK_PHASE1:
+		if (ctl)
+			g_phase1<true>(a, loc, lc, la, gd.t0, mt);
 		else
-			g_dense1<2>(a, loc, lc, la, mt);
+			g_phase1<false>(a, loc, lc, la, gd.t0, mt);
 		break;
 	case DK_GK_ANTI1:
 		if (gd.t0 == 0)
@@ -341,8 +405,8 @@ template <int N> __device__ __forceinline__ void cp_async_wait()
  * per thread (the 3 pass bits) into registers, applies the pass's gates and
  * scatters them back; the last read-out streams the tile to `out`.  The sum
  * of |amp|^2 read (touched tiles) and written goes to per-block partials. */
-template <typename R, int M, int SW>
-__global__ void __launch_bounds__(1 << (M - 3), 1)
+template <typename R, int M, int SW, int MINB>
+__global__ void __launch_bounds__(1 << (M - 3), MINB)
 	k_sweep(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
 		const unsigned char *__restrict__ prog, double *partials)
 {
@@ -898,6 +962,27 @@ unsigned long long g_launches = 0;
 
 /* ---------------------------------------------------------------------- */
 
+template <typename R, int M, int SW, int MINB>
+static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dprog,
+			     int m, size_t smem, int num_sms, uint64_t ntiles,
+			     const Scratch &s, cudaStream_t st, int *blocks_out)
+{
+	typedef typename CT<R>::T C2;
+	auto kern = k_sweep<R, M, SW, MINB>;
+	cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+					     (int)smem);
+	if (e != cudaSuccess)
+		return e;
+	uint64_t blocks = ntiles;
+	const uint64_t cap = (uint64_t)num_sms * MINB;
+	if (blocks > cap)
+		blocks = cap;
+	kern<<<(int)blocks, 1 << (m - 3), smem, st>>>((const C2 *)in, (C2 *)out, dprog,
+						     s.partials);
+	*blocks_out = (int)blocks;
+	return cudaSuccess;
+}
+
 cudaError_t launch_sweep(int prec, const void *in, void *out,
 			 const unsigned char *dprog, const dk_sweep_hdr *hp,
 			 const dk_scal *sc_in, dk_scal *sc_out, const Scratch &s,
@@ -905,34 +990,31 @@ cudaError_t launch_sweep(int prec, const void *in, void *out,
 {
 	g_num_sms = num_sms;
 	const int m = hp->m;
-	const int threads = 1 << (m - 3);
 	const size_t pass_bytes = ((size_t)hp->npass * sizeof(dk_pass_desc) + 15) & ~(size_t)15;
 	const size_t gate_bytes = (size_t)hp->ngate * sizeof(dk_gate_desc);
-	uint64_t blocks64 = hp->ntiles;
-	const uint64_t cap = (uint64_t)num_sms;
-	if (blocks64 > cap)
-		blocks64 = cap;
-	const int blocks = (int)blocks64;
+	/* 12-bit tiles: one 512-thread CTA per SM; up to 11 bits: two 256-thread
+	 * CTAs per SM.  Each CTA double-buffers its tile. */
+	int blocks = 0;
 	cudaError_t e;
 	if (prec == DK_C128) {
 		const size_t smem = ((size_t)32 << m) + pass_bytes + gate_bytes;
-		auto kern = k_sweep<double, DK_TILE_BITS_C128, 3>;
-		e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-					 (int)smem);
-		if (e != cudaSuccess)
-			return e;
-		kern<<<blocks, threads, smem, st>>>((const double2 *)in, (double2 *)out,
-						   dprog, s.partials);
+		if (m >= 12)
+			e = run_sweep<double, 12, 3, 1>(in, out, dprog, m, smem, num_sms,
+						       hp->ntiles, s, st, &blocks);
+		else
+			e = run_sweep<double, 11, 3, 2>(in, out, dprog, m, smem, num_sms,
+						       hp->ntiles, s, st, &blocks);
 	} else {
 		const size_t smem = ((size_t)16 << m) + pass_bytes + gate_bytes;
-		auto kern = k_sweep<float, DK_TILE_BITS_C64, 4>;
-		e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-					 (int)smem);
-		if (e != cudaSuccess)
-			return e;
-		kern<<<blocks, threads, smem, st>>>((const float2 *)in, (float2 *)out,
-						   dprog, s.partials);
+		if (m >= 12)
+			e = run_sweep<float, 12, 4, 1>(in, out, dprog, m, smem, num_sms,
+						      hp->ntiles, s, st, &blocks);
+		else
+			e = run_sweep<float, 11, 4, 2>(in, out, dprog, m, smem, num_sms,
+						      hp->ntiles, s, st, &blocks);
 	}
+	if (e != cudaSuccess)
+		return e;
 	const int all = hp->all_touched || (in != out);
 	k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc_in, sc_out, FIN_GATE, all);
 	g_launches += 2;

@@ -27,6 +27,8 @@ static int popc(uint64_t x) { return __builtin_popcountll(x); }
 void dk_plan_default_limits(int prec, unsigned n, dk_plan_limits *lim)
 {
 	int m = (prec == DK_C64) ? DK_TILE_BITS_C64 : DK_TILE_BITS_C128;
+	if (lim->tile_bits >= DK_PASS_BITS && lim->tile_bits <= 12)
+		m = lim->tile_bits; /* caller's choice */
 	if ((int)n < m)
 		m = (int)n;
 	lim->tile_bits = m;
@@ -52,10 +54,17 @@ int dk_gate_classify(const struct dk_gate *g)
 				offzero &= z;
 		}
 	if (g->k == 1) {
-		if (offzero)
+		const double *m = g->m;
+		if (offzero) {
+			if (m[0] == 1.0 && m[1] == 0.0)
+				return DK_GK_PHASE1;
 			return DK_GK_DIAG1;
-		if (diagzero)
+		}
+		if (diagzero) {
+			if (m[2] == 1.0 && m[3] == 0.0 && m[4] == 1.0 && m[5] == 0.0)
+				return DK_GK_SWAP1;
 			return DK_GK_ANTI1;
+		}
 		return DK_GK_DENSE1;
 	}
 	if (offzero)
@@ -82,6 +91,10 @@ static uint64_t target_mask(const dk_flat_op *op)
 static int mat_entries(int kind, unsigned k)
 {
 	switch (kind) {
+	case DK_GK_SWAP1:
+		return 0;
+	case DK_GK_PHASE1:
+		return 1;
 	case DK_GK_DIAG1:
 	case DK_GK_ANTI1:
 		return 2;
@@ -294,6 +307,11 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		const uint64_t d = op->gate->dim;
 		double *dst = mats + 2 * moff;
 		switch (kind) {
+		case DK_GK_SWAP1:
+			break;
+		case DK_GK_PHASE1:
+			memcpy(dst, src + 2 * 3, 16);
+			break;
 		case DK_GK_DIAG1:
 			memcpy(dst, src, 16);
 			memcpy(dst + 2, src + 2 * 3, 16);

@@ -36,6 +36,7 @@ struct Ctx {
 	size_t allocated = 0;
 	size_t budget = 0; /* 0 = unlimited */
 	int fuse = 1;
+	int tile_bits = 0; /* 0: planner default */
 	unsigned long long sweeps = 0, gates = 0, h2d = 0, d2h = 0;
 	std::recursive_mutex mu;
 	char err[256] = { 0 };
@@ -201,7 +202,8 @@ int flush(dk_state *s)
 			f.am = o->am;
 		}
 	}
-	dk_plan_limits lim;
+	dk_plan_limits lim = {};
+	lim.tile_bits = g.tile_bits;
 	dk_plan_default_limits(prec, n, &lim);
 	lim.fuse = g.fuse;
 	dk_plan plan;
@@ -437,6 +439,9 @@ int dk_init(int device)
 	CK(cudaMalloc(&g.scratch.marg, 64 * sizeof(double)));
 	const char *b = getenv("DK_HBM_BUDGET_BYTES");
 	g.budget = b ? (size_t)strtoull(b, nullptr, 10) : 0;
+	const char *tb = getenv("DK_TILE_BITS");
+	if (tb)
+		g.tile_bits = atoi(tb);
 	const char *f = getenv("DK_FUSE");
 	if (f)
 		g.fuse = atoi(f) ? 1 : 0;

@@ -149,6 +149,10 @@ def replay_sweep(blob, off, psi):
                     mat = np.array([[0, mats[mo]], [mats[mo + 1], 0]])
                 elif kind == 6:
                     mat = np.diag(mats[mo:mo + (1 << k)])
+                elif kind == 7:
+                    mat = np.array([[0, 1], [1, 0]], dtype=complex)
+                elif kind == 8:
+                    mat = np.diag([1, mats[mo]])
                 else:
                     raise AssertionError(kind)
                 tile = apply_local(tile, mat, tb, ok)
@@ -188,8 +192,10 @@ def random_ops(rng, n, count, kmax=3):
         r = rng.random()
         if k == 1 and r < 0.2:
             m = W.X.copy()
-        elif k == 1 and r < 0.4:
+        elif k == 1 and r < 0.3:
             m = np.diag(np.exp(2j * np.pi * rng.random(2)))
+        elif k == 1 and r < 0.4:
+            m = np.diag([1, np.exp(2j * np.pi * rng.random())])
         elif k == 2 and r < 0.3:
             m = np.diag(np.exp(2j * np.pi * rng.random(4)))
         else:

@@ -102,13 +102,20 @@ typedef struct dk_gate_desc {
 	uint32_t pad3;
 } dk_gate_desc; /* 40 bytes */
 
+/* A pass: the gates [g0, g1) applied to the 8 amplitudes each thread
+ * gathers from the shared tile.  The tile is stored under an XOR swizzle that
+ * is linear over GF(2), so a thread's 8 slots are
+ *   (slo[tid & 31] ^ shi[tid >> 5]) ^ (XOR of sp[j] over the set bits j of r),
+ * and the raw tile index (for control predicates) is the same with rlo, rhi,
+ * pm and OR.  The host precomputes these tables per pass. */
 typedef struct dk_pass_desc {
-	uint8_t b[DK_PASS_BITS]; /* local bit of register bit j */
-	uint8_t nlane;
-	uint8_t lane[16]; /* local bit of thread-index bit j */
 	uint16_t g0, g1; /* gate range [g0, g1) */
-	uint32_t pad;
-} dk_pass_desc; /* 28 bytes -> padded */
+	uint32_t flags; /* bit 0: a gate of the pass has controls inside the tile */
+	uint32_t sp[DK_PASS_BITS]; /* swizzled slot offset of pass bit j */
+	uint32_t pm[DK_PASS_BITS]; /* raw tile-index mask of pass bit j */
+	uint32_t slo[32], shi[16]; /* swizzled offsets of thread bits 0-4 / 5-8 */
+	uint32_t rlo[32], rhi[16]; /* raw tile-index bits of the same */
+} dk_pass_desc; /* 416 bytes */
 
 typedef struct dk_sweep_hdr {
 	int32_t m; /* tile bits */

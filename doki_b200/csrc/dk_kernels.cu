@@ -86,21 +86,37 @@ __device__ __forceinline__ bool ctl_ok(uint32_t loc, uint32_t lc, uint32_t la)
 }
 
 /* ---- gate application on the 8 register amplitudes of a pass ------------
- * a[r] holds the amplitude whose pass bits equal r; loc[r] is its tile
- * index (for local control predicates).  t_m: register bit of gate bit m. */
+ * A pass gathers, per thread, the NA = 2^PB amplitudes that differ only in the
+ * pass's PB tile bits: a[r] holds the one whose pass bits equal r, and
+ * loc(r) = gb | (pass bits of r) is its tile index, needed only to evaluate
+ * controls that lie inside the tile.  Template T / T0, T1 give the register
+ * bit that carries gate bit 0 / 1, so every register index is a compile-time
+ * constant and the amplitudes never leave registers. */
+constexpr int PB = DK_PASS_BITS;
+constexpr int NA = 1 << PB;
+
+static_assert(DK_PASS_BITS == 3, "register tile of 8 amplitudes");
+
+struct PassCtx {
+	uint32_t gb, p0, p1, p2; /* raw tile index of the thread part / pass bits */
+};
+
+__device__ __forceinline__ uint32_t loc_of(const PassCtx &c, int r)
+{
+	return c.gb | ((r & 1) ? c.p0 : 0u) | ((r & 2) ? c.p1 : 0u) | ((r & 4) ? c.p2 : 0u);
+}
 
 template <int T, bool CTL, typename C2>
-__device__ __forceinline__ void g_dense1(C2 (&a)[8], const uint32_t (&loc)[8],
-					 uint32_t lc, uint32_t la, const double2 *mt)
+__device__ __forceinline__ void g_dense1(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
+					 uint32_t la, const C2 *mt)
 {
-	const C2 m00 = ldm<C2>(mt), m01 = ldm<C2>(mt + 1);
-	const C2 m10 = ldm<C2>(mt + 2), m11 = ldm<C2>(mt + 3);
+	const C2 m00 = mt[0], m01 = mt[1], m10 = mt[2], m11 = mt[3];
 #pragma unroll
-	for (int r = 0; r < 8; ++r) {
+	for (int r = 0; r < NA; ++r) {
 		if (r & (1 << T))
 			continue;
 		const int r1 = r | (1 << T);
-		if (!CTL || ctl_ok(loc[r], lc, la)) {
+		if (!CTL || ctl_ok(loc_of(pc, r), lc, la)) {
 			const C2 x = a[r], y = a[r1];
 			a[r] = cmad(m01, y, cmul(m00, x));
 			a[r1] = cmad(m11, y, cmul(m10, x));
@@ -108,35 +124,17 @@ __device__ __forceinline__ void g_dense1(C2 (&a)[8], const uint32_t (&loc)[8],
 	}
 }
 
-template <int T, typename C2>
-__device__ __forceinline__ void g_anti1(C2 (&a)[8], const uint32_t (&loc)[8],
-					uint32_t lc, uint32_t la, const double2 *mt)
-{
-	const C2 m01 = ldm<C2>(mt), m10 = ldm<C2>(mt + 1);
-#pragma unroll
-	for (int r = 0; r < 8; ++r) {
-		if (r & (1 << T))
-			continue;
-		const int r1 = r | (1 << T);
-		if (ctl_ok(loc[r], lc, la)) {
-			const C2 x = a[r], y = a[r1];
-			a[r] = cmul(m01, y);
-			a[r1] = cmul(m10, x);
-		}
-	}
-}
-
 /* [[0,1],[1,0]] (X and its controlled forms): a pure exchange */
 template <int T, bool CTL, typename C2>
-__device__ __forceinline__ void g_swap1(C2 (&a)[8], const uint32_t (&loc)[8],
-					uint32_t lc, uint32_t la)
+__device__ __forceinline__ void g_swap1(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
+					uint32_t la)
 {
 #pragma unroll
-	for (int r = 0; r < 8; ++r) {
+	for (int r = 0; r < NA; ++r) {
 		if (r & (1 << T))
 			continue;
 		const int r1 = r | (1 << T);
-		if (!CTL || ctl_ok(loc[r], lc, la)) {
+		if (!CTL || ctl_ok(loc_of(pc, r), lc, la)) {
 			const C2 x = a[r];
 			a[r] = a[r1];
 			a[r1] = x;
@@ -144,195 +142,157 @@ __device__ __forceinline__ void g_swap1(C2 (&a)[8], const uint32_t (&loc)[8],
 	}
 }
 
-/* diag(1, d) (Z, S, T, phase and their controlled forms): scale |1> only */
-template <bool CTL, typename C2>
-__device__ __forceinline__ void g_phase1(C2 (&a)[8], const uint32_t (&loc)[8],
-					 uint32_t lc, uint32_t la, int t,
-					 const double2 *mt)
+template <int T, bool CTL, typename C2>
+__device__ __forceinline__ void g_anti1(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
+					uint32_t la, const C2 *mt)
 {
-	const C2 d1 = ldm<C2>(mt);
+	const C2 m01 = mt[0], m10 = mt[1];
 #pragma unroll
-	for (int r = 0; r < 8; ++r)
-		if (((r >> t) & 1) && (!CTL || ctl_ok(loc[r], lc, la)))
+	for (int r = 0; r < NA; ++r) {
+		if (r & (1 << T))
+			continue;
+		const int r1 = r | (1 << T);
+		if (!CTL || ctl_ok(loc_of(pc, r), lc, la)) {
+			const C2 x = a[r], y = a[r1];
+			a[r] = cmul(m01, y);
+			a[r1] = cmul(m10, x);
+		}
+	}
+}
+
+/* diag(1, d) (Z, S, T, phase and their controlled forms): scale |1> only */
+template <int T, bool CTL, typename C2>
+__device__ __forceinline__ void g_phase1(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
+					 uint32_t la, const C2 *mt)
+{
+	const C2 d1 = mt[0];
+#pragma unroll
+	for (int r = 0; r < NA; ++r)
+		if ((r & (1 << T)) && (!CTL || ctl_ok(loc_of(pc, r), lc, la)))
 			a[r] = cmul(d1, a[r]);
 }
 
-template <typename C2>
-__device__ __forceinline__ void g_diag1(C2 (&a)[8], const uint32_t (&loc)[8],
-					uint32_t lc, uint32_t la, int t,
-					const double2 *mt)
+template <int T, bool CTL, typename C2>
+__device__ __forceinline__ void g_diag1(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
+					uint32_t la, const C2 *mt)
 {
-	const C2 d0 = ldm<C2>(mt), d1 = ldm<C2>(mt + 1);
+	const C2 d0 = mt[0], d1 = mt[1];
 #pragma unroll
-	for (int r = 0; r < 8; ++r)
-		if (ctl_ok(loc[r], lc, la))
-			a[r] = cmul(((r >> t) & 1) ? d1 : d0, a[r]);
+	for (int r = 0; r < NA; ++r)
+		if (!CTL || ctl_ok(loc_of(pc, r), lc, la))
+			a[r] = cmul((r & (1 << T)) ? d1 : d0, a[r]);
 }
 
+/* diagonal gate on 2 or 3 targets (runtime register bits) */
 template <typename C2>
-__device__ __forceinline__ void g_diagk(C2 (&a)[8], const uint32_t (&loc)[8],
-					uint32_t lc, uint32_t la, int k, int t0,
-					int t1, int t2, const double2 *mt)
+__device__ __forceinline__ void g_diagk(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
+					uint32_t la, int k, int t0, int t1, int t2,
+					const C2 *mt)
 {
 #pragma unroll
-	for (int r = 0; r < 8; ++r) {
-		int gi = (r >> t0) & 1;
-		if (k > 1)
-			gi |= ((r >> t1) & 1) << 1;
+	for (int r = 0; r < NA; ++r) {
+		int gi = ((r >> t0) & 1) | (((r >> t1) & 1) << 1);
 		if (k > 2)
 			gi |= ((r >> t2) & 1) << 2;
-		if (ctl_ok(loc[r], lc, la))
-			a[r] = cmul(ldm<C2>(mt + gi), a[r]);
+		if (ctl_ok(loc_of(pc, r), lc, la))
+			a[r] = cmul(mt[gi], a[r]);
 	}
 }
 
 template <int T0, int T1, typename C2>
-__device__ __forceinline__ void g_dense2(C2 (&a)[8], const uint32_t (&loc)[8],
-					 uint32_t lc, uint32_t la, const double2 *mt)
+__device__ __forceinline__ void g_dense2(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
+					 uint32_t la, const C2 *mt)
 {
-	constexpr int R = 3 - T0 - T1;
 #pragma unroll
-	for (int h = 0; h < 2; ++h) {
-		const int b = h << R;
-		const int i0 = b, i1 = b | (1 << T0), i2 = b | (1 << T1),
-			  i3 = b | (1 << T0) | (1 << T1);
-		if (!ctl_ok(loc[b], lc, la))
+	for (int r = 0; r < NA; ++r) {
+		if (r & ((1 << T0) | (1 << T1)))
 			continue;
-		const C2 x0 = a[i0], x1 = a[i1], x2 = a[i2], x3 = a[i3];
+		const int i1 = r | (1 << T0), i2 = r | (1 << T1), i3 = i1 | (1 << T1);
+		if (!ctl_ok(loc_of(pc, r), lc, la))
+			continue;
+		const C2 x0 = a[r], x1 = a[i1], x2 = a[i2], x3 = a[i3];
 		C2 y[4];
 #pragma unroll
 		for (int row = 0; row < 4; ++row) {
-			C2 s = cmul(ldm<C2>(mt + 4 * row), x0);
-			s = cmad(ldm<C2>(mt + 4 * row + 1), x1, s);
-			s = cmad(ldm<C2>(mt + 4 * row + 2), x2, s);
-			y[row] = cmad(ldm<C2>(mt + 4 * row + 3), x3, s);
+			C2 s = cmul(mt[4 * row], x0);
+			s = cmad(mt[4 * row + 1], x1, s);
+			s = cmad(mt[4 * row + 2], x2, s);
+			y[row] = cmad(mt[4 * row + 3], x3, s);
 		}
-		a[i0] = y[0];
+		a[r] = y[0];
 		a[i1] = y[1];
 		a[i2] = y[2];
 		a[i3] = y[3];
 	}
 }
 
-template <int T0, int T1, int T2, typename C2>
-__device__ __forceinline__ void g_dense3(C2 (&a)[8], const uint32_t (&loc)[8],
-					 uint32_t lc, uint32_t la, const double2 *mt)
+template <bool CTL, typename C2>
+__device__ __forceinline__ void apply_1q(C2 (&a)[NA], const PassCtx &pc, int kind, int t0,
+					 uint32_t lc, uint32_t la, const C2 *mt)
 {
-	if (!ctl_ok(loc[0], lc, la))
-		return;
-	C2 x[8];
-#pragma unroll
-	for (int g = 0; g < 8; ++g)
-		x[g] = a[((g & 1) << T0) | (((g >> 1) & 1) << T1) | ((g >> 2) << T2)];
-#pragma unroll
-	for (int row = 0; row < 8; ++row) {
-		C2 s = cmul(ldm<C2>(mt + 8 * row), x[0]);
-#pragma unroll
-		for (int c = 1; c < 8; ++c)
-			s = cmad(ldm<C2>(mt + 8 * row + c), x[c], s);
-		a[((row & 1) << T0) | (((row >> 1) & 1) << T1) | ((row >> 2) << T2)] = s;
-	}
-}
-
-template <typename C2>
-__device__ __forceinline__ void g_dense3_any(C2 (&a)[8], const uint32_t (&loc)[8],
-					  uint32_t lc, uint32_t la, int t0, int t1,
-					  const double2 *mt)
-{
-	/* t2 is implied: the three register bits are a permutation */
-	if (t0 == 0 && t1 == 1)
-		g_dense3<0, 1, 2>(a, loc, lc, la, mt);
-	else if (t0 == 0)
-		g_dense3<0, 2, 1>(a, loc, lc, la, mt);
-	else if (t0 == 1 && t1 == 0)
-		g_dense3<1, 0, 2>(a, loc, lc, la, mt);
-	else if (t0 == 1)
-		g_dense3<1, 2, 0>(a, loc, lc, la, mt);
-	else if (t1 == 0)
-		g_dense3<2, 0, 1>(a, loc, lc, la, mt);
-	else
-		g_dense3<2, 1, 0>(a, loc, lc, la, mt);
-}
-
-template <typename C2>
-__device__ __forceinline__ void apply_gate(C2 (&a)[8], const uint32_t (&loc)[8],
-					   const dk_gate_desc &gd, const double2 *mats)
-{
-	const double2 *mt = mats + gd.mat;
-	const uint32_t lc = gd.lc, la = gd.la;
-	const bool ctl = (lc | la) != 0;
-	switch (gd.kind) {
+	switch (kind) {
 	case DK_GK_DENSE1:
-		if (ctl) {
-			if (gd.t0 == 0)
-				g_dense1<0, true>(a, loc, lc, la, mt);
-			else if (gd.t0 == 1)
-				g_dense1<1, true>(a, loc, lc, la, mt);
-			else
-				g_dense1<2, true>(a, loc, lc, la, mt);
-		} else {
-			if (gd.t0 == 0)
-				g_dense1<0, false>(a, loc, lc, la, mt);
-			else if (gd.t0 == 1)
-				g_dense1<1, false>(a, loc, lc, la, mt);
-			else
-				g_dense1<2, false>(a, loc, lc, la, mt);
+		switch (t0) {
+		case 0: g_dense1<0, CTL>(a, pc, lc, la, mt); break;
+		case 1: g_dense1<1, CTL>(a, pc, lc, la, mt); break;
+		default: g_dense1<2, CTL>(a, pc, lc, la, mt); break;
 		}
 		break;
 	case DK_GK_SWAP1:
-		if (ctl) {
-			if (gd.t0 == 0)
-				g_swap1<0, true>(a, loc, lc, la);
-			else if (gd.t0 == 1)
-				g_swap1<1, true>(a, loc, lc, la);
-			else
-				g_swap1<2, true>(a, loc, lc, la);
-		} else {
-			if (gd.t0 == 0)
-				g_swap1<0, false>(a, loc, lc, la);
-			else if (gd.t0 == 1)
-				g_swap1<1, false>(a, loc, lc, la);
-			else
-				g_swap1<2, false>(a, loc, lc, la);
+		switch (t0) {
+		case 0: g_swap1<0, CTL>(a, pc, lc, la); break;
+		case 1: g_swap1<1, CTL>(a, pc, lc, la); break;
+		default: g_swap1<2, CTL>(a, pc, lc, la); break;
 		}
 		break;
 	case DK_GK_PHASE1:
-		if (ctl)
-			g_phase1<true>(a, loc, lc, la, gd.t0, mt);
-		else
-			g_phase1<false>(a, loc, lc, la, gd.t0, mt);
-		break;
-	case DK_GK_ANTI1:
-		if (gd.t0 == 0)
-			g_anti1<0>(a, loc, lc, la, mt);
-		else if (gd.t0 == 1)
-			g_anti1<1>(a, loc, lc, la, mt);
-		else
-			g_anti1<2>(a, loc, lc, la, mt);
-		break;
-	case DK_GK_DIAG1:
-		g_diag1(a, loc, lc, la, gd.t0, mt);
-		break;
-	case DK_GK_DIAGK:
-		g_diagk(a, loc, lc, la, gd.k, gd.t0, gd.t1, gd.t2, mt);
-		break;
-	case DK_GK_DENSE2: {
-		const int c = gd.t0 * 3 + gd.t1;
-		switch (c) {
-		case 1: g_dense2<0, 1>(a, loc, lc, la, mt); break;
-		case 2: g_dense2<0, 2>(a, loc, lc, la, mt); break;
-		case 3: g_dense2<1, 0>(a, loc, lc, la, mt); break;
-		case 5: g_dense2<1, 2>(a, loc, lc, la, mt); break;
-		case 6: g_dense2<2, 0>(a, loc, lc, la, mt); break;
-		default: g_dense2<2, 1>(a, loc, lc, la, mt); break;
+		switch (t0) {
+		case 0: g_phase1<0, CTL>(a, pc, lc, la, mt); break;
+		case 1: g_phase1<1, CTL>(a, pc, lc, la, mt); break;
+		default: g_phase1<2, CTL>(a, pc, lc, la, mt); break;
 		}
 		break;
-	}
-	case DK_GK_DENSE3:
-		g_dense3_any(a, loc, lc, la, gd.t0, gd.t1, mt);
+	case DK_GK_DIAG1:
+		switch (t0) {
+		case 0: g_diag1<0, CTL>(a, pc, lc, la, mt); break;
+		case 1: g_diag1<1, CTL>(a, pc, lc, la, mt); break;
+		default: g_diag1<2, CTL>(a, pc, lc, la, mt); break;
+		}
+		break;
+	case DK_GK_ANTI1:
+		switch (t0) {
+		case 0: g_anti1<0, CTL>(a, pc, lc, la, mt); break;
+		case 1: g_anti1<1, CTL>(a, pc, lc, la, mt); break;
+		default: g_anti1<2, CTL>(a, pc, lc, la, mt); break;
+		}
 		break;
 	default:
 		break;
+	}
+}
+
+template <typename C2>
+__device__ __forceinline__ void apply_gate(C2 (&a)[NA], const PassCtx &pc,
+					   const dk_gate_desc &gd, const C2 *mats)
+{
+	const C2 *mt = mats + gd.mat;
+	const uint32_t lc = gd.lc, la = gd.la;
+	const int kind = gd.kind;
+	if (kind == DK_GK_DENSE2) {
+		switch (gd.t0 * 3 + gd.t1) {
+		case 1: g_dense2<0, 1>(a, pc, lc, la, mt); break;
+		case 2: g_dense2<0, 2>(a, pc, lc, la, mt); break;
+		case 3: g_dense2<1, 0>(a, pc, lc, la, mt); break;
+		case 5: g_dense2<1, 2>(a, pc, lc, la, mt); break;
+		case 6: g_dense2<2, 0>(a, pc, lc, la, mt); break;
+		default: g_dense2<2, 1>(a, pc, lc, la, mt); break;
+		}
+	} else if (kind == DK_GK_DIAGK) {
+		g_diagk(a, pc, lc, la, gd.k, gd.t0, gd.t1, gd.t2, mt);
+	} else if ((lc | la) != 0) {
+		apply_1q<true>(a, pc, kind, gd.t0, lc, la, mt);
+	} else {
+		apply_1q<false>(a, pc, kind, gd.t0, lc, la, mt);
 	}
 }
 
@@ -393,20 +353,19 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
 	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N> __device__ __forceinline__ void cp_async_wait()
-{
-	asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
-/* One CTA per SM streams tiles of 2^m amplitudes (index bits = the sweep's
- * qubit set, lowest qubits first so each tile is made of contiguous runs)
- * through two shared-memory buffers: while tile t is processed, tile t+grid
- * is already being copied in with cp.async.  Each pass gathers 8 amplitudes
- * per thread (the 3 pass bits) into registers, applies the pass's gates and
- * scatters them back; the last read-out streams the tile to `out`.  The sum
- * of |amp|^2 read (touched tiles) and written goes to per-block partials. */
-template <typename R, int M, int SW, int MINB>
-__global__ void __launch_bounds__(1 << (M - 3), MINB)
+/* Tiles of 2^m amplitudes (index bits = the sweep's qubit set, lowest
+ * qubits first so a tile is made of contiguous runs) stream through shared
+ * memory: cp.async brings a tile in, each pass gathers 8 amplitudes per thread
+ * into registers, applies the pass's gates and scatters them back, and the
+ * read-out streams the tile to `out`.  NBUF = 2: the next tile is copied into
+ * the second buffer while this one is processed (one CTA per SM); NBUF = 1:
+ * the next copy starts as soon as the read-out frees the buffer, overlapping
+ * the global stores (two CTAs per SM).  Sums of |amp|^2 read (touched tiles)
+ * and written go to per-block partials for the renormalisation. */
+template <typename R, int SW, int M, int MINB, int NBUF>
+__global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 	k_sweep(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
 		const unsigned char *__restrict__ prog, double *partials)
 {
@@ -414,41 +373,48 @@ __global__ void __launch_bounds__(1 << (M - 3), MINB)
 	extern __shared__ __align__(16) unsigned char sm[];
 	const dk_sweep_hdr *h = reinterpret_cast<const dk_sweep_hdr *>(prog);
 	const int m = h->m;
-	const int lanes = m - 3;
+	const int lanes = m - PB;
 	const uint32_t tid = threadIdx.x;
 	const int npass = h->npass, ngate = h->ngate;
-	const size_t tile_bytes = (size_t)sizeof(C2) << m;
-	const size_t pass_bytes = ((size_t)npass * sizeof(dk_pass_desc) + 15) & ~(size_t)15;
-	C2 *buf0 = reinterpret_cast<C2 *>(sm);
-	C2 *buf1 = reinterpret_cast<C2 *>(sm + tile_bytes);
-	dk_pass_desc *sp = reinterpret_cast<dk_pass_desc *>(sm + 2 * tile_bytes);
-	dk_gate_desc *sg = reinterpret_cast<dk_gate_desc *>(sm + 2 * tile_bytes + pass_bytes);
+	const int nmat = (int)((h->bytes - h->mat_off) / 16);
+	const uint32_t tn_amp = 1u << m;
+	const size_t gate_bytes = ((size_t)ngate * sizeof(dk_gate_desc) + 15) & ~(size_t)15;
+	C2 *bufs = reinterpret_cast<C2 *>(sm);
+	dk_gate_desc *sg = reinterpret_cast<dk_gate_desc *>(sm + NBUF * sizeof(C2) * tn_amp);
+	C2 *smat = reinterpret_cast<C2 *>(reinterpret_cast<unsigned char *>(sg) + gate_bytes);
+	const dk_pass_desc *passes = reinterpret_cast<const dk_pass_desc *>(prog + h->pass_off);
 	__shared__ uint8_t sq[16];
+	__shared__ uint64_t soff[NA]; /* global offset of register bits (load / store) */
+	__shared__ uint32_t sro[NA]; /* swizzled slot offset of the same */
 
-	{ /* stage the pass / gate tables and the tile bit positions */
-		const uint32_t *src = reinterpret_cast<const uint32_t *>(prog + h->pass_off);
-		uint32_t *dst = reinterpret_cast<uint32_t *>(sp);
-		const int nw = (int)(npass * sizeof(dk_pass_desc) / 4);
-		for (int i = tid; i < nw; i += blockDim.x)
-			dst[i] = __ldg(src + i);
-		src = reinterpret_cast<const uint32_t *>(prog + h->gate_off);
-		dst = reinterpret_cast<uint32_t *>(sg);
+	{ /* stage gates and matrices (in amplitude precision) */
+		const uint32_t *src = reinterpret_cast<const uint32_t *>(prog + h->gate_off);
+		uint32_t *dst = reinterpret_cast<uint32_t *>(sg);
 		const int gw = (int)(ngate * sizeof(dk_gate_desc) / 4);
 		for (int i = tid; i < gw; i += blockDim.x)
 			dst[i] = __ldg(src + i);
+		const double2 *msrc = reinterpret_cast<const double2 *>(prog + h->mat_off);
+		for (int i = tid; i < nmat; i += blockDim.x)
+			smat[i] = from_c128<C2>(__ldg(msrc + i));
 		/* blocks can be narrower than 16 threads (registers below 7 qubits) */
 		for (int i = tid; i < 16; i += blockDim.x)
 			sq[i] = h->qpos[i];
 	}
 	__syncthreads();
-	const double2 *mats = reinterpret_cast<const double2 *>(prog + h->mat_off);
-
+	for (int r = tid; r < NA; r += blockDim.x) {
+		uint64_t o = 0;
+		for (int j = 0; j < PB; ++j)
+			if ((r >> j) & 1)
+				o |= 1ull << sq[lanes + j];
+		soff[r] = o;
+		sro[r] = swz<SW>((uint32_t)r << lanes);
+	}
 	uint64_t off_t = 0;
 	for (int j = 0; j < lanes; ++j)
 		if ((tid >> j) & 1u)
 			off_t |= 1ull << sq[j];
-	const uint64_t h0 = 1ull << sq[lanes], h1 = 1ull << sq[lanes + 1],
-		       h2 = 1ull << sq[lanes + 2];
+	const uint32_t stid = swz<SW>(tid);
+	__syncthreads();
 	const uint64_t ntiles = h->ntiles;
 	const bool skip_idle = (in == out) && !h->all_touched;
 
@@ -472,17 +438,15 @@ __global__ void __launch_bounds__(1 << (M - 3), MINB)
 		}
 		return ntiles;
 	};
-	auto prefetch = [&](uint64_t t, C2 *buf) {
-		const uint64_t base = tile_base(t) | off_t;
+	auto prefetch = [&](uint64_t base, C2 *buf) {
+		const uint64_t bo = base | off_t;
 #pragma unroll
-		for (int r = 0; r < 8; ++r) {
-			const uint64_t gi = base | ((r & 1) ? h0 : 0) | ((r & 2) ? h1 : 0) |
-					    ((r & 4) ? h2 : 0);
-			C2 *dst = buf + swz<SW>(tid + ((uint32_t)r << lanes));
+		for (int r = 0; r < NA; ++r) {
+			C2 *dst = buf + (stid ^ sro[r]);
 			if (sizeof(C2) == 16)
-				cp_async16(dst, in + gi);
+				cp_async16(dst, in + (bo | soff[r]));
 			else
-				cp_async8(dst, in + gi);
+				cp_async8(dst, in + (bo | soff[r]));
 		}
 		cp_async_commit();
 	};
@@ -490,68 +454,85 @@ __global__ void __launch_bounds__(1 << (M - 3), MINB)
 	double insq = 0.0, outsq = 0.0;
 	uint64_t t = next_tile(blockIdx.x);
 	if (t < ntiles)
-		prefetch(t, buf0);
+		prefetch(tile_base(t), bufs);
 	int cur = 0;
 	while (t < ntiles) {
 		const uint64_t base = tile_base(t);
-		const uint64_t tn = next_tile(t + gridDim.x);
-		C2 *tile = cur ? buf1 : buf0;
-		if (tn < ntiles) {
-			prefetch(tn, cur ? buf0 : buf1);
-			cp_async_wait<1>();
+		C2 *tile = bufs + (NBUF == 2 ? cur * tn_amp : 0);
+		uint64_t tn = ntiles;
+		if (NBUF == 2) {
+			tn = next_tile(t + gridDim.x);
+			if (tn < ntiles) {
+				prefetch(tile_base(tn), bufs + (cur ^ 1) * tn_amp);
+				asm volatile("cp.async.wait_group 1;\n" ::);
+			} else {
+				cp_async_wait_all();
+			}
 		} else {
-			cp_async_wait<0>();
+			cp_async_wait_all();
 		}
 		__syncthreads();
-		C2 a[8];
+		C2 a[NA];
 		for (int p = 0; p < npass; ++p) {
-			const dk_pass_desc &pd = sp[p];
-			uint32_t gb = 0;
-			for (int j = 0; j < lanes; ++j)
-				gb |= ((tid >> j) & 1u) << pd.lane[j];
-			const uint32_t p0 = 1u << pd.b[0], p1 = 1u << pd.b[1],
-				       p2 = 1u << pd.b[2];
-			uint32_t loc[8];
+			const dk_pass_desc *pd = passes + p;
+			const uint32_t sgb = __ldg(&pd->slo[tid & 31]) ^ __ldg(&pd->shi[tid >> 5]);
+			const uint32_t s0 = __ldg(&pd->sp[0]), s1 = __ldg(&pd->sp[1]),
+				       s2 = __ldg(&pd->sp[2]);
+			uint32_t slot[NA];
 #pragma unroll
-			for (int r = 0; r < 8; ++r)
-				loc[r] = gb | ((r & 1) ? p0 : 0) | ((r & 2) ? p1 : 0) |
-					 ((r & 4) ? p2 : 0);
+			for (int r = 0; r < NA; ++r)
+				slot[r] = sgb ^ ((r & 1) ? s0 : 0u) ^ ((r & 2) ? s1 : 0u) ^
+					  ((r & 4) ? s2 : 0u);
 #pragma unroll
-			for (int r = 0; r < 8; ++r)
-				a[r] = tile[swz<SW>(loc[r])];
+			for (int r = 0; r < NA; ++r)
+				a[r] = tile[slot[r]];
 			if (p == 0) {
 #pragma unroll
-				for (int r = 0; r < 8; ++r)
+				for (int r = 0; r < NA; ++r)
 					insq += sqabs(a[r]);
 			}
-			const int g1 = pd.g1;
-			for (int g = pd.g0; g < g1; ++g) {
+			PassCtx pc;
+			if (__ldg(&pd->flags) & 1u) {
+				pc.gb = __ldg(&pd->rlo[tid & 31]) | __ldg(&pd->rhi[tid >> 5]);
+				pc.p0 = __ldg(&pd->pm[0]);
+				pc.p1 = __ldg(&pd->pm[1]);
+				pc.p2 = __ldg(&pd->pm[2]);
+			} else {
+				pc.gb = pc.p0 = pc.p1 = pc.p2 = 0;
+			}
+			const int g1 = __ldg(&pd->g1);
+			for (int g = __ldg(&pd->g0); g < g1; ++g) {
 				const dk_gate_desc &gd = sg[g];
-				if (((base & gd.gc) != gd.gc) || (base & gd.ga))
+				if ((gd.gc | gd.ga) && (((base & gd.gc) != gd.gc) || (base & gd.ga)))
 					continue;
-				apply_gate(a, loc, gd, mats);
+				apply_gate(a, pc, gd, smat);
 			}
 #pragma unroll
-			for (int r = 0; r < 8; ++r)
-				tile[swz<SW>(loc[r])] = a[r];
+			for (int r = 0; r < NA; ++r)
+				tile[slot[r]] = a[r];
 			__syncthreads();
 		}
 #pragma unroll
-		for (int r = 0; r < 8; ++r)
-			a[r] = tile[swz<SW>(tid + ((uint32_t)r << lanes))];
-		__syncthreads(); /* the buffer is refilled by the next prefetch */
+		for (int r = 0; r < NA; ++r)
+			a[r] = tile[stid ^ sro[r]];
+		if (NBUF == 1) {
+			__syncthreads(); /* the buffer is free: start the next tile's copy */
+			tn = next_tile(t + gridDim.x);
+			if (tn < ntiles)
+				prefetch(tile_base(tn), bufs);
+		}
 		const uint64_t bo = base | off_t;
 #pragma unroll
-		for (int r = 0; r < 8; ++r) {
-			const uint64_t gi = bo | ((r & 1) ? h0 : 0) | ((r & 2) ? h1 : 0) |
-					    ((r & 4) ? h2 : 0);
+		for (int r = 0; r < NA; ++r) {
 			outsq += sqabs(a[r]);
-			__stcs(out + gi, a[r]);
+			__stcs(out + (bo | soff[r]), a[r]);
 		}
+		if (NBUF == 2)
+			__syncthreads(); /* this buffer is refilled two tiles later */
 		t = tn;
 		cur ^= 1;
 	}
-	cp_async_wait<0>();
+	cp_async_wait_all();
 	block_sum2(insq, outsq);
 	if (tid == 0) {
 		partials[2 * blockIdx.x] = insq;
@@ -962,25 +943,29 @@ unsigned long long g_launches = 0;
 
 /* ---------------------------------------------------------------------- */
 
-template <typename R, int M, int SW, int MINB>
+template <typename R, int SW, int M, int MINB, int NBUF>
 static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dprog,
-			     int m, size_t smem, int num_sms, uint64_t ntiles,
-			     const Scratch &s, cudaStream_t st, int *blocks_out)
+			     const dk_sweep_hdr *hp, int num_sms, const Scratch &s,
+			     cudaStream_t st, int *blocks_out)
 {
 	typedef typename CT<R>::T C2;
-	auto kern = k_sweep<R, M, SW, MINB>;
+	const int m = hp->m;
+	const int nmat = (int)((hp->bytes - hp->mat_off) / 16);
+	const size_t gate_bytes = ((size_t)hp->ngate * sizeof(dk_gate_desc) + 15) & ~(size_t)15;
+	const size_t smem = NBUF * (sizeof(C2) << m) + gate_bytes + sizeof(C2) * (size_t)nmat;
+	auto kern = k_sweep<R, SW, M, MINB, NBUF>;
 	cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 					     (int)smem);
 	if (e != cudaSuccess)
 		return e;
-	uint64_t blocks = ntiles;
+	uint64_t blocks = hp->ntiles;
 	const uint64_t cap = (uint64_t)num_sms * MINB;
 	if (blocks > cap)
 		blocks = cap;
-	kern<<<(int)blocks, 1 << (m - 3), smem, st>>>((const C2 *)in, (C2 *)out, dprog,
-						     s.partials);
+	kern<<<(int)blocks, 1 << (m - DK_PASS_BITS), smem, st>>>((const C2 *)in, (C2 *)out,
+								   dprog, s.partials);
 	*blocks_out = (int)blocks;
-	return cudaSuccess;
+	return cudaGetLastError();
 }
 
 cudaError_t launch_sweep(int prec, const void *in, void *out,
@@ -990,29 +975,20 @@ cudaError_t launch_sweep(int prec, const void *in, void *out,
 {
 	g_num_sms = num_sms;
 	const int m = hp->m;
-	const size_t pass_bytes = ((size_t)hp->npass * sizeof(dk_pass_desc) + 15) & ~(size_t)15;
-	const size_t gate_bytes = (size_t)hp->ngate * sizeof(dk_gate_desc);
-	/* 12-bit tiles: one 512-thread CTA per SM; up to 11 bits: two 256-thread
-	 * CTAs per SM.  Each CTA double-buffers its tile. */
 	int blocks = 0;
 	cudaError_t e;
-	if (prec == DK_C128) {
-		const size_t smem = ((size_t)32 << m) + pass_bytes + gate_bytes;
-		if (m >= 12)
-			e = run_sweep<double, 12, 3, 1>(in, out, dprog, m, smem, num_sms,
-						       hp->ntiles, s, st, &blocks);
-		else
-			e = run_sweep<double, 11, 3, 2>(in, out, dprog, m, smem, num_sms,
-						       hp->ntiles, s, st, &blocks);
-	} else {
-		const size_t smem = ((size_t)16 << m) + pass_bytes + gate_bytes;
-		if (m >= 12)
-			e = run_sweep<float, 12, 4, 1>(in, out, dprog, m, smem, num_sms,
-						      hp->ntiles, s, st, &blocks);
-		else
-			e = run_sweep<float, 11, 4, 2>(in, out, dprog, m, smem, num_sms,
-						      hp->ntiles, s, st, &blocks);
-	}
+	/* 12-bit tiles: one 512-thread CTA per SM, double-buffered; up to 11 bits:
+	 * two 256-thread CTAs per SM, one buffer each */
+	if (prec == DK_C128)
+		e = m >= 12 ? run_sweep<double, 3, 12, 1, 2>(in, out, dprog, hp, num_sms, s, st,
+							     &blocks)
+			    : run_sweep<double, 3, 11, 2, 1>(in, out, dprog, hp, num_sms, s, st,
+							     &blocks);
+	else
+		e = m >= 12 ? run_sweep<float, 4, 12, 1, 2>(in, out, dprog, hp, num_sms, s, st,
+							    &blocks)
+			    : run_sweep<float, 4, 11, 2, 1>(in, out, dprog, hp, num_sms, s, st,
+							    &blocks);
 	if (e != cudaSuccess)
 		return e;
 	const int all = hp->all_touched || (in != out);

@@ -15,7 +15,8 @@
  * thread, the 8 amplitudes that differ in 3 chosen tile bits into registers
  * and applies every gate of the pass whose targets lie in those bits.
  *
- * Gates on more than 3 qubits become generic single-gate steps.
+ * Gates on more than 3 qubits, and dense (non-diagonal) 3-qubit gates, become
+ * generic single-gate steps.
  */
 #include <stdlib.h>
 #include <string.h>
@@ -131,7 +132,7 @@ static size_t align_up(size_t x, size_t a) { return (x + a - 1) & ~(a - 1); }
  * lowest `res` thread bits land on tile bits with pairwise distinct residues
  * mod `res` (then the XOR swizzle of the shared tile makes each quarter-warp
  * (complex128) / half-warp (complex64) access bank-conflict free). */
-static void lane_map(int m, const uint8_t *pb, int res, uint8_t *lane)
+static int lane_map(int m, const uint8_t *pb, int res, uint8_t *lane)
 {
 	int used[64] = { 0 };
 	int free_bits[64], nf = 0, nl = 0;
@@ -153,6 +154,43 @@ static void lane_map(int m, const uint8_t *pb, int res, uint8_t *lane)
 	for (int i = 0; i < nf; i++)
 		if (!taken[i])
 			lane[nl++] = (uint8_t)free_bits[i];
+	return nl;
+}
+
+/* The tile swizzle (must equal the kernel's swz<SW>): the low SW bits of the
+ * slot are XORed with every higher SW-bit group. */
+static uint32_t swizzle(uint32_t i, int sw)
+{
+	uint32_t f = 0;
+	for (int s = sw; s < 20; s += sw)
+		f ^= i >> s;
+	return i ^ (f & ((1u << sw) - 1u));
+}
+
+static void pass_tables(dk_pass_desc *pd, const uint8_t *pb, int m, int sw)
+{
+	uint8_t lane[32];
+	const int nl = lane_map(m, pb, sw, lane);
+	for (int j = 0; j < DK_PASS_BITS; j++) {
+		pd->pm[j] = 1u << pb[j];
+		pd->sp[j] = swizzle(pd->pm[j], sw);
+	}
+	for (uint32_t x = 0; x < 32; x++) {
+		uint32_t raw = 0;
+		for (int j = 0; j < 5 && j < nl; j++)
+			if ((x >> j) & 1u)
+				raw |= 1u << lane[j];
+		pd->rlo[x] = raw;
+		pd->slo[x] = swizzle(raw, sw);
+	}
+	for (uint32_t y = 0; y < 16; y++) {
+		uint32_t raw = 0;
+		for (int j = 0; j < 4 && 5 + j < nl; j++)
+			if ((y >> j) & 1u)
+				raw |= 1u << lane[5 + j];
+		pd->rhi[y] = raw;
+		pd->shi[y] = swizzle(raw, sw);
+	}
 }
 
 /* Emit one sweep program for ops[idx[0..cnt)] over tile set Q. */
@@ -178,11 +216,14 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	int *order = (int *)malloc(sizeof(int) * (cnt ? cnt : 1));
 	dk_pass_desc *passes =
 		(dk_pass_desc *)calloc((size_t)(cnt ? cnt : 1), sizeof(dk_pass_desc));
-	if (!rem || !defer || !order || !passes) {
+	uint8_t(*pbits)[DK_PASS_BITS] =
+		(uint8_t(*)[DK_PASS_BITS])calloc((size_t)(cnt ? cnt : 1), DK_PASS_BITS);
+	if (!rem || !defer || !order || !passes || !pbits) {
 		free(rem);
 		free(defer);
 		free(order);
 		free(passes);
+		free(pbits);
 		return -1;
 	}
 	int nrem = cnt, npass = 0, nord = 0;
@@ -215,15 +256,19 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 			}
 		}
 		pd->g1 = (uint16_t)nord;
-		/* fill the pass up to 3 bits with the highest free tile bits */
+		/* fill the pass up to DK_PASS_BITS bits with the highest free tile bits */
 		for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
 			P |= 1u << bit;
 		int j = 0;
 		for (int bit = 0; bit < m; bit++)
 			if (P & (1u << bit))
-				pd->b[j++] = (uint8_t)bit;
-		pd->nlane = (uint8_t)(m - DK_PASS_BITS);
-		lane_map(m, pd->b, res, pd->lane);
+				pbits[npass][j++] = (uint8_t)bit;
+		pass_tables(pd, pbits[npass], m, res);
+		for (int g = pd->g0; g < pd->g1; g++) {
+			const dk_flat_op *op = &ops[order[g]];
+			if ((op->cm | op->am) & Q)
+				pd->flags |= 1u;
+		}
 		npass++;
 		memcpy(rem, defer, sizeof(int) * (size_t)nd);
 		nrem = nd;
@@ -244,6 +289,7 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		free(defer);
 		free(order);
 		free(passes);
+		free(pbits);
 		return -1;
 	}
 	memset(b->p + b->len, 0, (start - b->len) + bytes);
@@ -269,7 +315,6 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	for (int i = 0; i < nord; i++) {
 		while (pi < npass && i >= passes[pi].g1)
 			pi++;
-		const dk_pass_desc *pd = &passes[pi];
 		const dk_flat_op *op = &ops[order[i]];
 		const int kind = kinds[order[i]];
 		dk_gate_desc *g = &gd[i];
@@ -279,7 +324,7 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		for (unsigned t = 0; t < op->k; t++) {
 			int lb = loc_of[op->tg[t]];
 			for (int r = 0; r < DK_PASS_BITS; r++)
-				if (pd->b[r] == lb)
+				if (pbits[pi][r] == lb)
 					treg[t] = (uint8_t)r;
 		}
 		g->t0 = treg[0];
@@ -339,6 +384,7 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	free(defer);
 	free(order);
 	free(passes);
+	free(pbits);
 	return 0;
 }
 
@@ -363,6 +409,10 @@ int dk_plan_build(const dk_flat_op *ops, int nops, unsigned n, int prec,
 		kinds[i] = (ops[i].k <= DK_SWEEP_MAX_K && sweepable)
 				   ? dk_gate_classify(ops[i].gate)
 				   : 0;
+		/* dense 3-qubit gates run as generic steps (kept out of the
+		 * register budget of the sweep) */
+		if (kinds[i] == DK_GK_DENSE3)
+			kinds[i] = 0;
 	}
 	int nrem = nops, nsteps = 0;
 	while (nrem > 0) {

@@ -46,12 +46,13 @@ HDR = np.dtype([("m", "<i4"), ("n", "<i4"), ("npass", "<i4"), ("ngate", "<i4"),
                 ("all_touched", "<i4"), ("pad", "<i4"), ("ntiles", "<u8"),
                 ("qpos", "u1", 16), ("pass_off", "<u4"), ("gate_off", "<u4"),
                 ("mat_off", "<u4"), ("bytes", "<u4")])
-PASS = np.dtype([("b", "u1", 3), ("nlane", "u1"), ("lane", "u1", 16), ("g0", "<u2"),
-                 ("g1", "<u2"), ("pad", "<u4")])
+PASS = np.dtype([("g0", "<u2"), ("g1", "<u2"), ("flags", "<u4"), ("sp", "<u4", 3),
+                 ("pm", "<u4", 3), ("slo", "<u4", 32), ("shi", "<u4", 16),
+                 ("rlo", "<u4", 32), ("rhi", "<u4", 16)])
 GATE = np.dtype([("kind", "u1"), ("k", "u1"), ("t", "u1", 3), ("pad", "u1", 3),
                  ("lc", "<u4"), ("la", "<u4"), ("gc", "<u8"), ("ga", "<u8"),
                  ("mat", "<u4"), ("pad3", "<u4")])
-assert HDR.itemsize == 64 and PASS.itemsize == 28 and GATE.itemsize == 40
+assert HDR.itemsize == 64 and PASS.itemsize == 416 and GATE.itemsize == 40
 
 
 @pytest.fixture(scope="module")
@@ -139,7 +140,7 @@ def replay_sweep(blob, off, psi):
                 lc, la = int(g["lc"]), int(g["la"])
                 ok = ((local & lc) == lc) & ((local & la) == 0)
                 k = int(g["k"])
-                tb = [int(p["b"][int(g["t"][j])]) for j in range(k)]
+                tb = [int(p["pm"][int(g["t"][j])]).bit_length() - 1 for j in range(k)]
                 kind, mo = int(g["kind"]), int(g["mat"])
                 if kind == 1 or kind == 4 or kind == 5:
                     mat = mats[mo:mo + (1 << 2 * k)].reshape(1 << k, 1 << k)
@@ -239,3 +240,46 @@ def test_plan_scale_circuit_fusion_ratio(lib):
     assert nsweeps <= 3 * c.depth
     tot = sum(int(np.frombuffer(blob, HDR, 1, off)[0]["ngate"]) for _, off, _ in steps)
     assert tot == len(c.ops)
+
+
+def swizzle(i, sw):
+    f = 0
+    s = sw
+    while s < 20:
+        f ^= i >> s
+        s += sw
+    return i ^ (f & ((1 << sw) - 1))
+
+
+@pytest.mark.parametrize("prec,n", [(2, 12), (2, 20), (1, 16), (2, 9), (2, 5)])
+def test_pass_tables_address_every_slot_once(lib, prec, n):
+    """The kernel's shared-memory slots for (thread, register) pairs, taken from
+    the per-pass tables, cover the tile exactly once, agree with the swizzle
+    of the raw tile index, and give conflict-free quarter-warps where the
+    lane mapping allows it."""
+    ops = random_ops(W.rng_for(300 + n), n, 40)
+    steps, blob = build_plan(lib, ops, n, prec=prec)
+    sw = 4 if prec == 1 else 3
+    for kind, off, _ in steps:
+        if kind != 1:
+            continue
+        h = np.frombuffer(blob, HDR, 1, off)[0]
+        m = int(h["m"])
+        nthreads = 1 << (m - 3)
+        passes = np.frombuffer(blob, PASS, int(h["npass"]), off + int(h["pass_off"]))
+        for p in passes:
+            slots, raws = [], []
+            for tid in range(nthreads):
+                sg = int(p["slo"][tid & 31]) ^ int(p["shi"][tid >> 5])
+                rg = int(p["rlo"][tid & 31]) | int(p["rhi"][tid >> 5])
+                for r in range(8):
+                    sl, rw = sg, rg
+                    for j in range(3):
+                        if (r >> j) & 1:
+                            sl ^= int(p["sp"][j])
+                            rw |= int(p["pm"][j])
+                    assert swizzle(rw, sw) == sl
+                    slots.append(sl)
+                    raws.append(rw)
+            assert sorted(slots) == list(range(1 << m))
+            assert sorted(raws) == list(range(1 << m))

@@ -92,15 +92,38 @@ enum {
 	DK_GK_DIAGK = 6,
 	DK_GK_SWAP1 = 7, /* [[0,1],[1,0]]: exchange, no arithmetic */
 	DK_GK_PHASE1 = 8, /* diag(1, d): scale the |1> half only */
+	DK_GK_NEG1 = 9, /* diag(1, -1): negate the |1> half */
 };
 
+/* Gate descriptor of a sweep (16 bytes, one shared-memory load).  `code`
+ * selects the kernel's specialised entry: for the one-qubit kinds it is
+ * DK_GC_<KIND> + t0 + 3 * (has controls inside the tile); DK_GC_DENSE2 + the
+ * index of the ordered register-bit pair; DK_GC_DIAGK.  `info` keeps the
+ * kind (bits 8-11), k (6-7) and register bits t2 (4-5), t1 (2-3), t0 (0-1). */
 typedef struct dk_gate_desc {
-	uint8_t kind, k, t0, t1, t2, pad0, pad1, pad2; /* t_m: register bit of gate bit m */
+	uint16_t code;
+	uint16_t mat; /* offset of the matrix in complex entries */
+	uint16_t gcond; /* index into the global-condition table, 0xffff: none */
+	uint16_t info;
 	uint32_t lc, la; /* control / anticontrol masks over local (tile) bits */
-	uint64_t gc, ga; /* control / anticontrol masks over global bits */
-	uint32_t mat; /* offset of the matrix in complex entries */
-	uint32_t pad3;
-} dk_gate_desc; /* 40 bytes */
+} dk_gate_desc;
+
+/* Controls outside the tile: the gate acts on a tile iff
+ * (base & gc) == gc && !(base & ga) for the tile's base index. */
+typedef struct dk_gate_cond {
+	uint64_t gc, ga;
+} dk_gate_cond;
+
+enum {
+	DK_GC_DENSE1 = 0,
+	DK_GC_SWAP1 = 6,
+	DK_GC_PHASE1 = 12,
+	DK_GC_DIAG1 = 18,
+	DK_GC_ANTI1 = 24,
+	DK_GC_DENSE2 = 30, /* + pair index: (0,1) (0,2) (1,0) (1,2) (2,0) (2,1) */
+	DK_GC_DIAGK = 36,
+	DK_GC_NEG1 = 37,
+};
 
 /* A pass: the gates [g0, g1) applied to the 8 amplitudes each thread
  * gathers from the shared tile.  The tile is stored under an XOR swizzle that
@@ -127,6 +150,8 @@ typedef struct dk_sweep_hdr {
 	uint8_t qpos[16]; /* global bit of local bit j (ascending) */
 	uint32_t pass_off, gate_off, mat_off; /* byte offsets from the header */
 	uint32_t bytes; /* total program bytes */
+	uint32_t cond_off, ncond; /* global-condition table */
+	uint32_t pad2[2];
 } dk_sweep_hdr;
 
 /* One step of a flush plan. */

@@ -172,6 +172,17 @@ __device__ __forceinline__ void g_phase1(C2 (&a)[NA], const PassCtx &pc, uint32_
 			a[r] = cmul(d1, a[r]);
 }
 
+/* diag(1, -1) (Z, CZ and controlled forms): negate |1> only */
+template <int T, bool CTL, typename C2>
+__device__ __forceinline__ void g_neg1(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
+				       uint32_t la)
+{
+#pragma unroll
+	for (int r = 0; r < NA; ++r)
+		if ((r & (1 << T)) && (!CTL || ctl_ok(loc_of(pc, r), lc, la)))
+			a[r] = mk(-a[r].x, -a[r].y);
+}
+
 template <int T, bool CTL, typename C2>
 __device__ __forceinline__ void g_diag1(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
 					uint32_t la, const C2 *mt)
@@ -226,73 +237,59 @@ __device__ __forceinline__ void g_dense2(C2 (&a)[NA], const PassCtx &pc, uint32_
 	}
 }
 
-template <bool CTL, typename C2>
-__device__ __forceinline__ void apply_1q(C2 (&a)[NA], const PassCtx &pc, int kind, int t0,
-					 uint32_t lc, uint32_t la, const C2 *mt)
-{
-	switch (kind) {
-	case DK_GK_DENSE1:
-		switch (t0) {
-		case 0: g_dense1<0, CTL>(a, pc, lc, la, mt); break;
-		case 1: g_dense1<1, CTL>(a, pc, lc, la, mt); break;
-		default: g_dense1<2, CTL>(a, pc, lc, la, mt); break;
-		}
-		break;
-	case DK_GK_SWAP1:
-		switch (t0) {
-		case 0: g_swap1<0, CTL>(a, pc, lc, la); break;
-		case 1: g_swap1<1, CTL>(a, pc, lc, la); break;
-		default: g_swap1<2, CTL>(a, pc, lc, la); break;
-		}
-		break;
-	case DK_GK_PHASE1:
-		switch (t0) {
-		case 0: g_phase1<0, CTL>(a, pc, lc, la, mt); break;
-		case 1: g_phase1<1, CTL>(a, pc, lc, la, mt); break;
-		default: g_phase1<2, CTL>(a, pc, lc, la, mt); break;
-		}
-		break;
-	case DK_GK_DIAG1:
-		switch (t0) {
-		case 0: g_diag1<0, CTL>(a, pc, lc, la, mt); break;
-		case 1: g_diag1<1, CTL>(a, pc, lc, la, mt); break;
-		default: g_diag1<2, CTL>(a, pc, lc, la, mt); break;
-		}
-		break;
-	case DK_GK_ANTI1:
-		switch (t0) {
-		case 0: g_anti1<0, CTL>(a, pc, lc, la, mt); break;
-		case 1: g_anti1<1, CTL>(a, pc, lc, la, mt); break;
-		default: g_anti1<2, CTL>(a, pc, lc, la, mt); break;
-		}
-		break;
-	default:
-		break;
-	}
-}
-
+/* One gate of a pass: a single jump on the host-computed entry code. */
 template <typename C2>
-__device__ __forceinline__ void apply_gate(C2 (&a)[NA], const PassCtx &pc,
-					   const dk_gate_desc &gd, const C2 *mats)
+__device__ __forceinline__ void apply_gate(C2 (&a)[NA], const PassCtx &pc, uint32_t code,
+					   uint32_t info, uint32_t lc, uint32_t la,
+					   const C2 *mt)
 {
-	const C2 *mt = mats + gd.mat;
-	const uint32_t lc = gd.lc, la = gd.la;
-	const int kind = gd.kind;
-	if (kind == DK_GK_DENSE2) {
-		switch (gd.t0 * 3 + gd.t1) {
-		case 1: g_dense2<0, 1>(a, pc, lc, la, mt); break;
-		case 2: g_dense2<0, 2>(a, pc, lc, la, mt); break;
-		case 3: g_dense2<1, 0>(a, pc, lc, la, mt); break;
-		case 5: g_dense2<1, 2>(a, pc, lc, la, mt); break;
-		case 6: g_dense2<2, 0>(a, pc, lc, la, mt); break;
-		default: g_dense2<2, 1>(a, pc, lc, la, mt); break;
-		}
-	} else if (kind == DK_GK_DIAGK) {
-		g_diagk(a, pc, lc, la, gd.k, gd.t0, gd.t1, gd.t2, mt);
-	} else if ((lc | la) != 0) {
-		apply_1q<true>(a, pc, kind, gd.t0, lc, la, mt);
-	} else {
-		apply_1q<false>(a, pc, kind, gd.t0, lc, la, mt);
+	switch (code) {
+	case DK_GC_DENSE1 + 0: g_dense1<0, false>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE1 + 1: g_dense1<1, false>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE1 + 2: g_dense1<2, false>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE1 + 3: g_dense1<0, true>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE1 + 4: g_dense1<1, true>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE1 + 5: g_dense1<2, true>(a, pc, lc, la, mt); break;
+	case DK_GC_SWAP1 + 0: g_swap1<0, false>(a, pc, lc, la); break;
+	case DK_GC_SWAP1 + 1: g_swap1<1, false>(a, pc, lc, la); break;
+	case DK_GC_SWAP1 + 2: g_swap1<2, false>(a, pc, lc, la); break;
+	case DK_GC_SWAP1 + 3: g_swap1<0, true>(a, pc, lc, la); break;
+	case DK_GC_SWAP1 + 4: g_swap1<1, true>(a, pc, lc, la); break;
+	case DK_GC_SWAP1 + 5: g_swap1<2, true>(a, pc, lc, la); break;
+	case DK_GC_PHASE1 + 0: g_phase1<0, false>(a, pc, lc, la, mt); break;
+	case DK_GC_PHASE1 + 1: g_phase1<1, false>(a, pc, lc, la, mt); break;
+	case DK_GC_PHASE1 + 2: g_phase1<2, false>(a, pc, lc, la, mt); break;
+	case DK_GC_PHASE1 + 3: g_phase1<0, true>(a, pc, lc, la, mt); break;
+	case DK_GC_PHASE1 + 4: g_phase1<1, true>(a, pc, lc, la, mt); break;
+	case DK_GC_PHASE1 + 5: g_phase1<2, true>(a, pc, lc, la, mt); break;
+	case DK_GC_DIAG1 + 0: g_diag1<0, false>(a, pc, lc, la, mt); break;
+	case DK_GC_DIAG1 + 1: g_diag1<1, false>(a, pc, lc, la, mt); break;
+	case DK_GC_DIAG1 + 2: g_diag1<2, false>(a, pc, lc, la, mt); break;
+	case DK_GC_DIAG1 + 3: g_diag1<0, true>(a, pc, lc, la, mt); break;
+	case DK_GC_DIAG1 + 4: g_diag1<1, true>(a, pc, lc, la, mt); break;
+	case DK_GC_DIAG1 + 5: g_diag1<2, true>(a, pc, lc, la, mt); break;
+	case DK_GC_ANTI1 + 0: g_anti1<0, false>(a, pc, lc, la, mt); break;
+	case DK_GC_ANTI1 + 1: g_anti1<1, false>(a, pc, lc, la, mt); break;
+	case DK_GC_ANTI1 + 2: g_anti1<2, false>(a, pc, lc, la, mt); break;
+	case DK_GC_ANTI1 + 3: g_anti1<0, true>(a, pc, lc, la, mt); break;
+	case DK_GC_ANTI1 + 4: g_anti1<1, true>(a, pc, lc, la, mt); break;
+	case DK_GC_ANTI1 + 5: g_anti1<2, true>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE2 + 0: g_dense2<0, 1>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE2 + 1: g_dense2<0, 2>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE2 + 2: g_dense2<1, 0>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE2 + 3: g_dense2<1, 2>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE2 + 4: g_dense2<2, 0>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE2 + 5: g_dense2<2, 1>(a, pc, lc, la, mt); break;
+	case DK_GC_NEG1 + 0: g_neg1<0, false>(a, pc, lc, la); break;
+	case DK_GC_NEG1 + 1: g_neg1<1, false>(a, pc, lc, la); break;
+	case DK_GC_NEG1 + 2: g_neg1<2, false>(a, pc, lc, la); break;
+	case DK_GC_NEG1 + 3: g_neg1<0, true>(a, pc, lc, la); break;
+	case DK_GC_NEG1 + 4: g_neg1<1, true>(a, pc, lc, la); break;
+	case DK_GC_NEG1 + 5: g_neg1<2, true>(a, pc, lc, la); break;
+	default:
+		g_diagk(a, pc, lc, la, (info >> 6) & 3, info & 3, (info >> 2) & 3,
+			(info >> 4) & 3, mt);
+		break;
 	}
 }
 
@@ -378,21 +375,27 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 	const int npass = h->npass, ngate = h->ngate;
 	const int nmat = (int)((h->bytes - h->mat_off) / 16);
 	const uint32_t tn_amp = 1u << m;
-	const size_t gate_bytes = ((size_t)ngate * sizeof(dk_gate_desc) + 15) & ~(size_t)15;
+	const int ncond = (int)h->ncond;
+	const size_t gate_bytes = (size_t)ngate * sizeof(dk_gate_desc);
+	const size_t cond_bytes = (size_t)ncond * sizeof(dk_gate_cond);
 	C2 *bufs = reinterpret_cast<C2 *>(sm);
-	dk_gate_desc *sg = reinterpret_cast<dk_gate_desc *>(sm + NBUF * sizeof(C2) * tn_amp);
-	C2 *smat = reinterpret_cast<C2 *>(reinterpret_cast<unsigned char *>(sg) + gate_bytes);
+	uint4 *sg = reinterpret_cast<uint4 *>(sm + NBUF * sizeof(C2) * tn_amp);
+	dk_gate_cond *scond =
+		reinterpret_cast<dk_gate_cond *>(reinterpret_cast<unsigned char *>(sg) + gate_bytes);
+	C2 *smat = reinterpret_cast<C2 *>(reinterpret_cast<unsigned char *>(scond) + cond_bytes);
 	const dk_pass_desc *passes = reinterpret_cast<const dk_pass_desc *>(prog + h->pass_off);
 	__shared__ uint8_t sq[16];
 	__shared__ uint64_t soff[NA]; /* global offset of register bits (load / store) */
 	__shared__ uint32_t sro[NA]; /* swizzled slot offset of the same */
 
 	{ /* stage gates and matrices (in amplitude precision) */
-		const uint32_t *src = reinterpret_cast<const uint32_t *>(prog + h->gate_off);
-		uint32_t *dst = reinterpret_cast<uint32_t *>(sg);
-		const int gw = (int)(ngate * sizeof(dk_gate_desc) / 4);
-		for (int i = tid; i < gw; i += blockDim.x)
-			dst[i] = __ldg(src + i);
+		const uint4 *src = reinterpret_cast<const uint4 *>(prog + h->gate_off);
+		for (int i = tid; i < ngate; i += blockDim.x)
+			sg[i] = __ldg(src + i);
+		const uint4 *csrc = reinterpret_cast<const uint4 *>(prog + h->cond_off);
+		uint4 *cdst = reinterpret_cast<uint4 *>(scond);
+		for (int i = tid; i < ncond; i += blockDim.x)
+			cdst[i] = __ldg(csrc + i);
 		const double2 *msrc = reinterpret_cast<const double2 *>(prog + h->mat_off);
 		for (int i = tid; i < nmat; i += blockDim.x)
 			smat[i] = from_c128<C2>(__ldg(msrc + i));
@@ -432,9 +435,14 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 			if (!skip_idle)
 				return t;
 			const uint64_t base = tile_base(t);
-			for (int g = 0; g < ngate; ++g)
-				if (((base & sg[g].gc) == sg[g].gc) && !(base & sg[g].ga))
+			for (int g = 0; g < ngate; ++g) {
+				const uint32_t gi = sg[g].y & 0xffffu;
+				if (gi == 0xffffu)
 					return t;
+				const dk_gate_cond c = scond[gi];
+				if (((base & c.gc) == c.gc) && !(base & c.ga))
+					return t;
+			}
 		}
 		return ntiles;
 	};
@@ -502,10 +510,14 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 			}
 			const int g1 = __ldg(&pd->g1);
 			for (int g = __ldg(&pd->g0); g < g1; ++g) {
-				const dk_gate_desc &gd = sg[g];
-				if ((gd.gc | gd.ga) && (((base & gd.gc) != gd.gc) || (base & gd.ga)))
-					continue;
-				apply_gate(a, pc, gd, smat);
+				const uint4 d = sg[g];
+				const uint32_t gi = d.y & 0xffffu;
+				if (gi != 0xffffu) {
+					const dk_gate_cond c = scond[gi];
+					if (((base & c.gc) != c.gc) || (base & c.ga))
+						continue;
+				}
+				apply_gate(a, pc, d.x & 0xffffu, d.y >> 16, d.z, d.w, smat + (d.x >> 16));
 			}
 #pragma unroll
 			for (int r = 0; r < NA; ++r)
@@ -951,8 +963,8 @@ static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dpr
 	typedef typename CT<R>::T C2;
 	const int m = hp->m;
 	const int nmat = (int)((hp->bytes - hp->mat_off) / 16);
-	const size_t gate_bytes = ((size_t)hp->ngate * sizeof(dk_gate_desc) + 15) & ~(size_t)15;
-	const size_t smem = NBUF * (sizeof(C2) << m) + gate_bytes + sizeof(C2) * (size_t)nmat;
+	const size_t smem = NBUF * (sizeof(C2) << m) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
+			    (size_t)hp->ncond * sizeof(dk_gate_cond) + sizeof(C2) * (size_t)nmat;
 	auto kern = k_sweep<R, SW, M, MINB, NBUF>;
 	cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 					     (int)smem);

@@ -57,6 +57,8 @@ int dk_gate_classify(const struct dk_gate *g)
 	if (g->k == 1) {
 		const double *m = g->m;
 		if (offzero) {
+			if (m[0] == 1.0 && m[1] == 0.0 && m[6] == -1.0 && m[7] == 0.0)
+				return DK_GK_NEG1;
 			if (m[0] == 1.0 && m[1] == 0.0)
 				return DK_GK_PHASE1;
 			return DK_GK_DIAG1;
@@ -93,6 +95,7 @@ static int mat_entries(int kind, unsigned k)
 {
 	switch (kind) {
 	case DK_GK_SWAP1:
+	case DK_GK_NEG1:
 		return 0;
 	case DK_GK_PHASE1:
 		return 1;
@@ -278,9 +281,16 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	int nmat = 0;
 	for (int i = 0; i < nord; i++)
 		nmat += mat_entries(kinds[order[i]], ops[order[i]].k);
+	int ncond = 0;
+	for (int i = 0; i < nord; i++) {
+		const dk_flat_op *op = &ops[order[i]];
+		if ((op->cm | op->am) & ~Q)
+			ncond++;
+	}
 	size_t pass_off = align_up(sizeof(dk_sweep_hdr), 16);
 	size_t gate_off = align_up(pass_off + sizeof(dk_pass_desc) * (size_t)npass, 16);
-	size_t mat_off = align_up(gate_off + sizeof(dk_gate_desc) * (size_t)nord, 16);
+	size_t cond_off = align_up(gate_off + sizeof(dk_gate_desc) * (size_t)nord, 16);
+	size_t mat_off = align_up(cond_off + sizeof(dk_gate_cond) * (size_t)ncond, 16);
 	size_t bytes = align_up(mat_off + 16 * (size_t)nmat, 16);
 
 	size_t start = align_up(b->len, 16);
@@ -306,11 +316,14 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	h->gate_off = (uint32_t)gate_off;
 	h->mat_off = (uint32_t)mat_off;
 	h->bytes = (uint32_t)bytes;
+	h->cond_off = (uint32_t)cond_off;
+	h->ncond = (uint32_t)ncond;
 	memcpy(base + pass_off, passes, sizeof(dk_pass_desc) * (size_t)npass);
 
 	dk_gate_desc *gd = (dk_gate_desc *)(base + gate_off);
+	dk_gate_cond *conds = (dk_gate_cond *)(base + cond_off);
 	double *mats = (double *)(base + mat_off);
-	int moff = 0, all_touched = 0;
+	int moff = 0, all_touched = 0, ci = 0;
 	int pi = 0;
 	for (int i = 0; i < nord; i++) {
 		while (pi < npass && i >= passes[pi].g1)
@@ -318,8 +331,6 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		const dk_flat_op *op = &ops[order[i]];
 		const int kind = kinds[order[i]];
 		dk_gate_desc *g = &gd[i];
-		g->kind = (uint8_t)kind;
-		g->k = (uint8_t)op->k;
 		uint8_t treg[3] = { 0, 0, 0 };
 		for (unsigned t = 0; t < op->k; t++) {
 			int lb = loc_of[op->tg[t]];
@@ -327,32 +338,54 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 				if (pbits[pi][r] == lb)
 					treg[t] = (uint8_t)r;
 		}
-		g->t0 = treg[0];
-		g->t1 = treg[1];
-		g->t2 = treg[2];
+		uint64_t gc = 0, ga = 0;
 		for (unsigned q = 0; q < n; q++) {
 			uint64_t bit = UINT64_C(1) << q;
 			if (op->cm & bit) {
 				if (loc_of[q] >= 0)
 					g->lc |= 1u << loc_of[q];
 				else
-					g->gc |= bit;
+					gc |= bit;
 			}
 			if (op->am & bit) {
 				if (loc_of[q] >= 0)
 					g->la |= 1u << loc_of[q];
 				else
-					g->ga |= bit;
+					ga |= bit;
 			}
 		}
-		if (g->gc == 0 && g->ga == 0)
+		if (gc == 0 && ga == 0) {
 			all_touched = 1;
-		g->mat = (uint32_t)moff;
+			g->gcond = 0xffff;
+		} else {
+			conds[ci].gc = gc;
+			conds[ci].ga = ga;
+			g->gcond = (uint16_t)ci++;
+		}
+		const int ctl = (g->lc | g->la) != 0;
+		switch (kind) {
+		case DK_GK_DENSE1: g->code = (uint16_t)(DK_GC_DENSE1 + treg[0] + 3 * ctl); break;
+		case DK_GK_SWAP1: g->code = (uint16_t)(DK_GC_SWAP1 + treg[0] + 3 * ctl); break;
+		case DK_GK_PHASE1: g->code = (uint16_t)(DK_GC_PHASE1 + treg[0] + 3 * ctl); break;
+		case DK_GK_DIAG1: g->code = (uint16_t)(DK_GC_DIAG1 + treg[0] + 3 * ctl); break;
+		case DK_GK_ANTI1: g->code = (uint16_t)(DK_GC_ANTI1 + treg[0] + 3 * ctl); break;
+		case DK_GK_NEG1: g->code = (uint16_t)(DK_GC_NEG1 + treg[0] + 3 * ctl); break;
+		case DK_GK_DENSE2: {
+			static const int pair_index[3][3] = { { -1, 0, 1 }, { 2, -1, 3 }, { 4, 5, -1 } };
+			g->code = (uint16_t)(DK_GC_DENSE2 + pair_index[treg[0]][treg[1]]);
+			break;
+		}
+		default: g->code = DK_GC_DIAGK; break;
+		}
+		g->info = (uint16_t)(treg[0] | (treg[1] << 2) | (treg[2] << 4) |
+				     ((op->k & 3u) << 6) | ((unsigned)kind << 8));
+		g->mat = (uint16_t)moff;
 		const double *src = op->gate->m;
 		const uint64_t d = op->gate->dim;
 		double *dst = mats + 2 * moff;
 		switch (kind) {
 		case DK_GK_SWAP1:
+		case DK_GK_NEG1:
 			break;
 		case DK_GK_PHASE1:
 			memcpy(dst, src + 2 * 3, 16);

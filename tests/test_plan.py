@@ -45,14 +45,15 @@ class Plan(ctypes.Structure):
 HDR = np.dtype([("m", "<i4"), ("n", "<i4"), ("npass", "<i4"), ("ngate", "<i4"),
                 ("all_touched", "<i4"), ("pad", "<i4"), ("ntiles", "<u8"),
                 ("qpos", "u1", 16), ("pass_off", "<u4"), ("gate_off", "<u4"),
-                ("mat_off", "<u4"), ("bytes", "<u4")])
+                ("mat_off", "<u4"), ("bytes", "<u4"), ("cond_off", "<u4"),
+                ("ncond", "<u4"), ("pad2", "<u4", 2)])
 PASS = np.dtype([("g0", "<u2"), ("g1", "<u2"), ("flags", "<u4"), ("sp", "<u4", 3),
                  ("pm", "<u4", 3), ("slo", "<u4", 32), ("shi", "<u4", 16),
                  ("rlo", "<u4", 32), ("rhi", "<u4", 16)])
-GATE = np.dtype([("kind", "u1"), ("k", "u1"), ("t", "u1", 3), ("pad", "u1", 3),
-                 ("lc", "<u4"), ("la", "<u4"), ("gc", "<u8"), ("ga", "<u8"),
-                 ("mat", "<u4"), ("pad3", "<u4")])
-assert HDR.itemsize == 64 and PASS.itemsize == 416 and GATE.itemsize == 40
+GATE = np.dtype([("code", "<u2"), ("mat", "<u2"), ("gcond", "<u2"), ("info", "<u2"),
+                 ("lc", "<u4"), ("la", "<u4")])
+COND = np.dtype([("gc", "<u8"), ("ga", "<u8")])
+assert HDR.itemsize == 80 and PASS.itemsize == 416 and GATE.itemsize == 16
 
 
 @pytest.fixture(scope="module")
@@ -113,12 +114,25 @@ def apply_local(vec, mat, tbits, ok):
     return out
 
 
+def assert_code(code, kind, treg, ctl):
+    """The kernel's entry code must agree with the gate's kind and bits."""
+    one_q = {1: 0, 7: 6, 8: 12, 2: 18, 3: 24, 9: 37}
+    if kind in one_q:
+        assert code == one_q[kind] + treg[0] + 3 * (ctl != 0)
+    elif kind == 4:
+        pairs = [(0, 1), (0, 2), (1, 0), (1, 2), (2, 0), (2, 1)]
+        assert code == 30 + pairs.index((treg[0], treg[1]))
+    else:
+        assert kind == 6 and code == 36
+
+
 def replay_sweep(blob, off, psi):
     h = np.frombuffer(blob, HDR, 1, off)[0]
     m, n = int(h["m"]), int(h["n"])
     qpos = [int(x) for x in h["qpos"][:m]]
     passes = np.frombuffer(blob, PASS, int(h["npass"]), off + int(h["pass_off"]))
     gates = np.frombuffer(blob, GATE, int(h["ngate"]), off + int(h["gate_off"]))
+    conds = np.frombuffer(blob, COND, int(h["ncond"]), off + int(h["cond_off"]))
     nmat = (int(h["bytes"]) - int(h["mat_off"])) // 16
     mats = np.frombuffer(blob, np.complex128, nmat, off + int(h["mat_off"]))
     qmask = sum(1 << q for q in qpos)
@@ -134,14 +148,19 @@ def replay_sweep(blob, off, psi):
         for p in passes:
             for gi in range(int(p["g0"]), int(p["g1"])):
                 g = gates[gi]
-                gc, ga = int(g["gc"]), int(g["ga"])
-                if (base & gc) != gc or (base & ga):
-                    continue
+                if int(g["gcond"]) != 0xffff:
+                    c = conds[int(g["gcond"])]
+                    gc, ga = int(c["gc"]), int(c["ga"])
+                    if (base & gc) != gc or (base & ga):
+                        continue
                 lc, la = int(g["lc"]), int(g["la"])
                 ok = ((local & lc) == lc) & ((local & la) == 0)
-                k = int(g["k"])
-                tb = [int(p["pm"][int(g["t"][j])]).bit_length() - 1 for j in range(k)]
-                kind, mo = int(g["kind"]), int(g["mat"])
+                info = int(g["info"])
+                k = (info >> 6) & 3
+                treg = [info & 3, (info >> 2) & 3, (info >> 4) & 3]
+                tb = [int(p["pm"][treg[j]]).bit_length() - 1 for j in range(k)]
+                kind, mo = info >> 8, int(g["mat"])
+                assert_code(int(g["code"]), kind, treg, lc | la)
                 if kind == 1 or kind == 4 or kind == 5:
                     mat = mats[mo:mo + (1 << 2 * k)].reshape(1 << k, 1 << k)
                 elif kind == 2:
@@ -154,6 +173,8 @@ def replay_sweep(blob, off, psi):
                     mat = np.array([[0, 1], [1, 0]], dtype=complex)
                 elif kind == 8:
                     mat = np.diag([1, mats[mo]])
+                elif kind == 9:
+                    mat = np.diag([1, -1]).astype(complex)
                 else:
                     raise AssertionError(kind)
                 tile = apply_local(tile, mat, tb, ok)
@@ -195,8 +216,10 @@ def random_ops(rng, n, count, kmax=3):
             m = W.X.copy()
         elif k == 1 and r < 0.3:
             m = np.diag(np.exp(2j * np.pi * rng.random(2)))
-        elif k == 1 and r < 0.4:
+        elif k == 1 and r < 0.35:
             m = np.diag([1, np.exp(2j * np.pi * rng.random())])
+        elif k == 1 and r < 0.4:
+            m = W.Z.copy()
         elif k == 2 and r < 0.3:
             m = np.diag(np.exp(2j * np.pi * rng.random(4)))
         else:

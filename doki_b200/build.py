@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "--expt-relaxed-constexpr", "-I", INC, "-I", CSRC]
 
-CU_SOURCES = ["dk_kernels.cu", "dk_runtime.cu"]
+CU_SOURCES = ["dk_kernels.cu", "dk_runtime.cu", "dk_noalloc.cu"]
 C_SOURCES = ["dk_plan.c"]
 HEADERS = ["dk_internal.h", "dk_kernels.h"]
 

@@ -1098,6 +1098,38 @@ cudaError_t launch_marginals(int prec, const void *d, unsigned n, const Scratch 
 	return cudaGetLastError();
 }
 
+cudaError_t launch_marginals_blocks(int prec, const void *d, unsigned n,
+				    const Scratch &s, int max_blocks, cudaStream_t st)
+{
+	int threads = 256, blocks = 1;
+	if (n < 8)
+		threads = 1 << n;
+	else {
+		int lb = (int)n - 8;
+		while (lb > 0 && (1 << lb) > max_blocks)
+			lb--;
+		blocks = 1 << lb;
+	}
+	int sbits = 0;
+	while ((1 << sbits) < threads * blocks)
+		sbits++;
+	if ((int)n - sbits > kMargHi)
+		return cudaErrorInvalidValue;
+	if (threads < 32) {
+		threads = 32;
+		sbits = (int)n;
+	}
+	if (prec == DK_C128)
+		k_marginals<double><<<blocks, threads, 0, st>>>((const double2 *)d,
+							       (int)n, sbits, s.partials);
+	else
+		k_marginals<float><<<blocks, threads, 0, st>>>((const float2 *)d,
+							      (int)n, sbits, s.partials);
+	k_marg_finalize<<<1, 64, 0, st>>>(s.partials, blocks, (int)n, s.marg);
+	g_launches += 2;
+	return cudaGetLastError();
+}
+
 cudaError_t launch_measure_collapse(int prec, const void *in, void *out,
 				    unsigned n, unsigned q, double roll,
 				    int forced, const dk_scal *sc_in,

@@ -49,6 +49,11 @@ cudaError_t launch_import(int prec, const double *src, void *d, unsigned n,
 cudaError_t launch_marginals(int prec, const void *d, unsigned n,
 			     const Scratch &s, cudaStream_t st);
 
+/* the same reduction with at most `max_blocks` (a power of two) blocks, for
+ * callers whose partials array holds only that many slots */
+cudaError_t launch_marginals_blocks(int prec, const void *d, unsigned n,
+				    const Scratch &s, int max_blocks, cudaStream_t st);
+
 /* decide outcome of qubit q against roll (uses s.marg), then gather the
  * selected half into out (n-1 qubits) */
 cudaError_t launch_measure_collapse(int prec, const void *in, void *out,

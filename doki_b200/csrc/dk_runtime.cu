@@ -404,6 +404,8 @@ const char *dk_strerror(int status)
 	case DK_ERR_EMPTY: return "registry has no qubits";
 	case DK_ERR_NORM0: return "New normalization constant is 0";
 	case DK_ERR_NODEV: return "no CUDA device available";
+	case DK_ERR_NOALLOC_LIMIT:
+		return "register exceeds the allocation-free entry point's maximum of 40 qubits";
 	default: return "unknown error";
 	}
 }

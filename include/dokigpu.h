@@ -42,6 +42,7 @@ extern "C" {
 #define DK_ERR_EMPTY 25 /* operation on a 0-qubit register */
 #define DK_ERR_NORM0 26 /* collapse produced a zero normalisation constant */
 #define DK_ERR_NODEV 27 /* no usable CUDA device */
+#define DK_ERR_NOALLOC_LIMIT 28 /* register larger than dk_marginals_noalloc handles */
 
 /* ---- precisions (reference platform.h:199 PRECISION 1 / 2) ------------ */
 #define DK_C64 1 /* complex64 amplitudes, FP64 norm / reductions */
@@ -156,6 +157,25 @@ int dk_state_flush(dk_state *s);
 /* The CUDA stream (cudaStream_t) all of this library's work is queued on,
  * for callers that time it with events; NULL before initialisation. */
 void *dk_stream(void);
+
+/* ---- allocation-free marginals (no counterpart in the reference) --------
+ * For callers that cannot let a library allocate device memory (a framework
+ * that owns every device byte through its own allocator or an HBM-budget
+ * arena, or a latency-critical loop where cudaMalloc / cudaFree would
+ * synchronise the device).  Same reduction as dk_marginals, on a caller-owned
+ * device array `amps` of 2^num_qubits amplitudes (complex64 or complex128 by
+ * `precision`), queued on `stream` (a cudaStream_t, NULL = default stream).
+ * Writes num_qubits + 1 doubles to the caller-owned device array `out`:
+ * out[q] = sum of |amps[i]|^2 over i with bit q set, out[num_qubits] = the
+ * sum over all i.  Allocates nothing: its scratch is a fixed 128 KiB array in
+ * every device that loads this library, held until the process exits.  The
+ * first call on a device looks that array's device address up (make it before
+ * any stream capture).  Calls share the array, so calls that overlap on the
+ * device race.  num_qubits above DK_NOALLOC_MAX_QUBITS returns
+ * DK_ERR_NOALLOC_LIMIT. */
+#define DK_NOALLOC_MAX_QUBITS 40
+int dk_marginals_noalloc(const void *amps, unsigned num_qubits, int precision,
+			 double *out, void *stream);
 
 #ifdef __cplusplus
 }

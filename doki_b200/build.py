@@ -25,9 +25,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "--expt-relaxed-constexpr", "-I", INC, "-I", CSRC]
 
-CU_SOURCES = ["dk_kernels.cu", "dk_runtime.cu", "dk_noalloc.cu"]
+CU_SOURCES = ["dk_kernels.cu", "dk_runtime.cu", "dk_noalloc.cu", "dk_batch.cu"]
 C_SOURCES = ["dk_plan.c"]
-HEADERS = ["dk_internal.h", "dk_kernels.h"]
+HEADERS = ["dk_internal.h", "dk_kernels.h", "dk_device.cuh"]
 
 LIB = os.path.join(HERE, "libdokigpu.so")
 EXT = os.path.join(HERE, "doki" + sysconfig.get_config_var("EXT_SUFFIX"))

@@ -79,8 +79,8 @@ struct dk_state {
 
 /* ---- fused sweep program (built on the host, read by the sweep kernel) -- */
 
-#define DK_TILE_BITS_C128 12
-#define DK_TILE_BITS_C64 12
+#define DK_TILE_BITS_C128 11
+#define DK_TILE_BITS_C64 11
 #define DK_PASS_BITS 3
 
 enum {

@@ -25,6 +25,9 @@
 
 static int popc(uint64_t x) { return __builtin_popcountll(x); }
 
+/* gates examined per pass when grouping a sweep's gates into passes */
+#define DK_PASS_WINDOW 64
+
 void dk_plan_default_limits(int prec, unsigned n, dk_plan_limits *lim)
 {
 	int m = (prec == DK_C64) ? DK_TILE_BITS_C64 : DK_TILE_BITS_C128;
@@ -242,7 +245,8 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		for (int i = 0; i < nrem; i++) {
 			const dk_flat_op *op = &ops[rem[i]];
 			uint64_t sup = support(op);
-			if (sup & blocked) {
+			/* bounded lookahead keeps grouping linear in the gate count */
+			if (i >= DK_PASS_WINDOW || (sup & blocked)) {
 				defer[nd++] = rem[i];
 				blocked |= sup;
 				continue;

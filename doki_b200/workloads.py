@@ -164,3 +164,116 @@ def run_ops(mod, reg, ops: Sequence[Op], gate_cache=None, num_threads=-1):
                                  num_threads, False)
         reg = new
     return reg
+
+
+@dataclass
+class FlatBatch:
+    """A batch of circuits as flat arrays (the layout of dk_batch_build)."""
+    num_qubits: np.ndarray  # uint32 [C]
+    keep: np.ndarray  # uint32 [C]
+    op_start: np.ndarray  # uint64 [C + 1]
+    op_k: np.ndarray  # uint32 [N]
+    op_targets: np.ndarray  # uint32 [N, 3]
+    op_controls: np.ndarray  # uint64 [N]
+    op_anticontrols: np.ndarray  # uint64 [N]
+    op_matrix: np.ndarray  # uint64 [N]: first complex entry of the op's matrix
+    matrices: np.ndarray  # complex128 [M]
+
+    @property
+    def count(self) -> int:
+        return int(self.num_qubits.size)
+
+    def ops(self, c: int) -> List[Op]:
+        """Circuit c as a list of Op (for the oracle and the plain path)."""
+        out = []
+        for i in range(int(self.op_start[c]), int(self.op_start[c + 1])):
+            k = int(self.op_k[i])
+            m0 = int(self.op_matrix[i])
+            mat = self.matrices[m0:m0 + (1 << (2 * k))].reshape(1 << k, 1 << k).copy()
+            cm, am = int(self.op_controls[i]), int(self.op_anticontrols[i])
+            out.append(Op(mat, [int(t) for t in self.op_targets[i, :k]],
+                          {q for q in range(64) if (cm >> q) & 1},
+                          {q for q in range(64) if (am >> q) & 1}))
+        return out
+
+    def subset(self, idx: Sequence[int]) -> "FlatBatch":
+        """The circuits idx as a batch of their own (shares matrices)."""
+        starts = [0]
+        sel = []
+        for c in idx:
+            a, b = int(self.op_start[c]), int(self.op_start[c + 1])
+            sel.append(np.arange(a, b))
+            starts.append(starts[-1] + (b - a))
+        ops = np.concatenate(sel) if sel else np.zeros(0, dtype=np.int64)
+        return FlatBatch(self.num_qubits[list(idx)].copy(), self.keep[list(idx)].copy(),
+                         np.array(starts, dtype=np.uint64), self.op_k[ops].copy(),
+                         self.op_targets[ops].copy(), self.op_controls[ops].copy(),
+                         self.op_anticontrols[ops].copy(), self.op_matrix[ops].copy(),
+                         self.matrices)
+
+
+def _u3_many(angles: np.ndarray) -> np.ndarray:
+    th, ph, la = angles[:, 0], angles[:, 1], angles[:, 2]
+    c, s = np.cos(th / 2.0), np.sin(th / 2.0)
+    m = np.empty((angles.shape[0], 2, 2), dtype=np.complex128)
+    m[:, 0, 0] = c
+    m[:, 0, 1] = -np.exp(1j * la) * s
+    m[:, 1, 0] = np.exp(1j * ph) * s
+    m[:, 1, 1] = np.exp(1j * (ph + la)) * c
+    return m
+
+
+def batch_arrays(seed: int = 4, count: int = 4096, qmin: int = 4, qmax: int = 16,
+                 dmin: int = 10, dmax: int = 50) -> FlatBatch:
+    """Batching form: `count` independent registers with n ~ U[qmin, qmax] and
+    depth ~ U[dmin, dmax]; each layer is U3(theta, phi, lambda ~ U[0, 2pi)) on
+    every qubit, then, on a random disjoint pairing, a CNOT or a controlled
+    U3 (probability 1/2 each).  The reduced density matrix is taken over the
+    lower floor(n / 2) qubits."""
+    rng = rng_for(seed)
+    ns = rng.integers(qmin, qmax + 1, size=count)
+    depths = rng.integers(dmin, dmax + 1, size=count)
+    mats = [X.reshape(-1)]  # entry 0..3: the shared X matrix
+    moff = 4
+    ks, tgs, cms, mat_idx, starts = [], [], [], [], [0]
+    for c in range(count):
+        n, d = int(ns[c]), int(depths[c])
+        npairs = n // 2
+        # per layer: n U3 on qubits 0..n-1, then npairs controlled ops
+        u3s = _u3_many(rng.random((d * n, 3)) * 2.0 * np.pi)
+        perms = np.argsort(rng.random((d, n)), axis=1)
+        coin = rng.random((d, npairs)) < 0.5
+        cu = _u3_many(rng.random((d * npairs, 3)) * 2.0 * np.pi)
+        layer_ops = n + npairs
+        tot = d * layer_ops
+        tg = np.zeros((tot, 3), dtype=np.uint32)
+        cm = np.zeros(tot, dtype=np.uint64)
+        mi = np.zeros(tot, dtype=np.uint64)
+        base = np.arange(d) * layer_ops
+        # U3 on every qubit
+        u_idx = (base[:, None] + np.arange(n)[None, :]).reshape(-1)
+        tg[u_idx, 0] = np.tile(np.arange(n, dtype=np.uint32), d)
+        mi[u_idx] = moff + 4 * np.arange(d * n, dtype=np.uint64)
+        mats.append(u3s.reshape(-1))
+        moff += 4 * d * n
+        # controlled ops on the pairing (control perm[2a], target perm[2a+1])
+        p_idx = (base[:, None] + n + np.arange(npairs)[None, :]).reshape(-1)
+        ctl = perms[:, 0:2 * npairs:2].reshape(-1)
+        tgt = perms[:, 1:2 * npairs:2].reshape(-1)
+        tg[p_idx, 0] = tgt.astype(np.uint32)
+        cm[p_idx] = (np.uint64(1) << ctl.astype(np.uint64))
+        flat_coin = coin.reshape(-1)
+        mi[p_idx] = np.where(flat_coin, 0,
+                             moff + 4 * np.arange(d * npairs, dtype=np.uint64)).astype(np.uint64)
+        mats.append(cu.reshape(-1))
+        moff += 4 * d * npairs
+        ks.append(np.ones(tot, dtype=np.uint32))
+        tgs.append(tg)
+        cms.append(cm)
+        mat_idx.append(mi)
+        starts.append(starts[-1] + tot)
+    n_ops = starts[-1]
+    return FlatBatch(ns.astype(np.uint32), (ns // 2).astype(np.uint32),
+                     np.array(starts, dtype=np.uint64), np.concatenate(ks),
+                     np.concatenate(tgs), np.concatenate(cms), np.zeros(n_ops, dtype=np.uint64),
+                     np.concatenate(mat_idx), np.concatenate(mats).astype(np.complex128))

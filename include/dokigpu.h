@@ -158,6 +158,44 @@ int dk_state_flush(dk_state *s);
  * for callers that time it with events; NULL before initialisation. */
 void *dk_stream(void);
 
+/* ---- batching form (no counterpart in the reference) --------------------
+ * Thousands of independent registers (4..16 qubits), each starting in |0..0>
+ * with its own gate sequence, run by one CUDA-graph launch.  Circuit c has
+ * num_qubits[c] qubits and ops op_start[c] .. op_start[c+1]-1; op i acts on
+ * op_k[i] <= 3 targets op_targets[3*i .. 3*i+k-1] (targets[0] = LSB of the
+ * gate index, as registry_apply), with control / anticontrol bit masks
+ * op_controls[i] / op_anticontrols[i], and its 2^k x 2^k row-major complex128
+ * matrix starts at complex entry op_matrix[i] of `matrices`.  Dense 3-qubit
+ * gates are not accepted (diagonal ones are).  After the circuit, each
+ * register's reduced density matrix over its lower keep_qubits[c] qubits
+ * (<= 12) is formed on the device, divided by its trace.  Registers above 12
+ * qubits stream through tiles of `tile_bits` (8..12) qubits. */
+typedef struct dk_batch dk_batch;
+int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qubits,
+		   const unsigned *keep_qubits, const uint64_t *op_start,
+		   const unsigned *op_k, const unsigned *op_targets,
+		   const uint64_t *op_controls, const uint64_t *op_anticontrols,
+		   const uint64_t *op_matrix, const double *matrices, int tile_bits,
+		   dk_batch **out);
+/* CTAs per SM for the batch kernels (1..4); the autotuner's second knob. */
+int dk_batch_set_ctas(dk_batch *b, int ctas_per_sm);
+/* Queue every circuit (captured into a CUDA graph on first use); keep_states
+ * also stores each final register for dk_batch_state.  Returns before the
+ * device finishes; see dk_batch_sync / dk_batch_stream. */
+int dk_batch_run(dk_batch *b, int keep_states);
+int dk_batch_sync(dk_batch *b);
+void *dk_batch_stream(dk_batch *b);
+/* reduced density matrix of circuit c: 2 * 4^keep doubles (row-major) */
+int dk_batch_rho(dk_batch *b, unsigned circuit, double *out);
+/* all reduced density matrices, concatenated; offsets[c] = first complex
+ * entry of circuit c (may be NULL) */
+int dk_batch_rho_all(dk_batch *b, double *out, uint64_t *offsets);
+uint64_t dk_batch_rho_elems(const dk_batch *b);
+/* final raw amplitudes of circuit c (needs keep_states): 2 * 2^n doubles */
+int dk_batch_state(dk_batch *b, unsigned circuit, double *out);
+const char *dk_batch_error(const dk_batch *b);
+void dk_batch_free(dk_batch *b);
+
 /* ---- allocation-free marginals (no counterpart in the reference) --------
  * For callers that cannot let a library allocate device memory (a framework
  * that owns every device byte through its own allocator or an HBM-budget

@@ -64,6 +64,7 @@ typedef struct dk_op {
 struct dk_state {
 	unsigned n;
 	int prec;
+	int slot; /* stream slot the register's work is queued on */
 	int released;
 	dk_buf *buf; /* NULL for 0-qubit registers */
 	dk_op *pending; /* ops queued on top of buf's content */

@@ -18,6 +18,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -26,28 +27,87 @@
 
 namespace {
 
-struct Ctx {
-	int inited = 0;
-	int device = 0;
-	int num_sms = 148;
+/* A slot: one CUDA stream with its own scratch and cuBLAS handle.  Every
+ * register belongs to the slot that created it (derived registers inherit
+ * it); work on a register is queued on its slot's stream under its slot's
+ * lock, so registers of different slots run concurrently on the device and a
+ * thread waiting for its results does not block other slots. */
+struct Slot {
 	cudaStream_t st = nullptr;
 	dk::Scratch scratch{};
 	cublasHandle_t blas = nullptr;
-	size_t allocated = 0;
+	std::recursive_mutex mu;
+};
+
+constexpr int kMaxSlots = 64;
+
+struct Ctx {
+	std::atomic<int> inited{ 0 };
+	int device = 0;
+	int num_sms = 148;
+	std::mutex init_mu;
+	std::mutex slots_mu;
+	Slot *slots[kMaxSlots] = { nullptr };
+	std::atomic<int> nslots{ 0 };
+	std::atomic<size_t> allocated{ 0 };
 	size_t budget = 0; /* 0 = unlimited */
 	int fuse = 1;
 	int tile_bits = 0; /* 0: planner default */
-	unsigned long long sweeps = 0, gates = 0, h2d = 0, d2h = 0;
-	std::recursive_mutex mu;
+	std::atomic<unsigned long long> sweeps{ 0 }, gates{ 0 }, h2d{ 0 }, d2h{ 0 };
 	char err[256] = { 0 };
 };
 
 Ctx g;
 
-struct Lock {
-	Lock() { g.mu.lock(); }
-	~Lock() { g.mu.unlock(); }
+/* slot new registers of this thread are created on */
+thread_local int t_slot = 0;
+/* slot of the operation in progress on this thread (set by SlotLock) */
+thread_local Slot *t_active = nullptr;
+#define CUR (*t_active)
+
+/* Locks a slot for the current scope and makes it the active one. */
+struct SlotLock {
+	Slot *prev;
+	Slot *sl;
+	explicit SlotLock(int id)
+	{
+		prev = t_active;
+		if (id < 0 || id >= kMaxSlots || !g.slots[id])
+			id = 0;
+		sl = g.slots[id];
+		if (sl) {
+			sl->mu.lock();
+			t_active = sl;
+		}
+	}
+	~SlotLock()
+	{
+		if (sl)
+			sl->mu.unlock();
+		t_active = prev;
+	}
 };
+
+int create_slot(int id)
+{
+	Slot *sl = new Slot();
+	cudaError_t e = cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking);
+	if (e == cudaSuccess)
+		e = cudaMalloc(&sl->scratch.partials,
+			       sizeof(double) * dk::kMaxBlocks * dk::kPartialStride);
+	if (e == cudaSuccess)
+		e = cudaMalloc(&sl->scratch.u64, 4 * sizeof(unsigned long long));
+	if (e == cudaSuccess)
+		e = cudaMalloc(&sl->scratch.marg, 64 * sizeof(double));
+	if (e != cudaSuccess) {
+		snprintf(g.err, sizeof(g.err), "%s", cudaGetErrorString(e));
+		cudaGetLastError();
+		delete sl;
+		return DK_ERR_CUDA;
+	}
+	g.slots[id] = sl;
+	return DK_OK;
+}
 
 int cuda_fail(cudaError_t e)
 {
@@ -65,7 +125,7 @@ int cuda_fail(cudaError_t e)
 
 int ensure_init()
 {
-	if (g.inited)
+	if (g.inited.load())
 		return DK_OK;
 	return dk_init(-1);
 }
@@ -74,9 +134,9 @@ size_t amp_bytes(int prec) { return prec == DK_C64 ? 8 : 16; }
 
 int dev_alloc(void **p, size_t bytes)
 {
-	if (g.budget && g.allocated + bytes > g.budget)
+	if (g.budget && g.allocated.load() + bytes > g.budget)
 		return DK_ERR_BUDGET;
-	cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, g.st);
+	cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, CUR.st);
 	if (e != cudaSuccess)
 		return cuda_fail(e);
 	g.allocated += bytes;
@@ -87,7 +147,7 @@ void dev_free(void *p, size_t bytes)
 {
 	if (!p)
 		return;
-	cudaFreeAsync(p, g.st);
+	cudaFreeAsync(p, CUR.st);
 	g.allocated -= bytes;
 }
 
@@ -116,7 +176,7 @@ int buf_new(unsigned n, int prec, dk_buf **out)
 		return rc;
 	}
 	/* pool memory is recycled: start every scalar block from zero */
-	cudaError_t e = cudaMemsetAsync(b->sc, 0, sizeof(dk_scal), g.st);
+	cudaError_t e = cudaMemsetAsync(b->sc, 0, sizeof(dk_scal), CUR.st);
 	if (e != cudaSuccess) {
 		buf_release(b);
 		return cuda_fail(e);
@@ -138,7 +198,7 @@ void buf_release(dk_buf *b)
 
 /* ---- pending op chains ------------------------------------------------- */
 
-void gate_retain(dk_gate *gt) { gt->refcount++; }
+void gate_retain(dk_gate *gt) { __atomic_fetch_add(&gt->refcount, 1, __ATOMIC_RELAXED); }
 
 void op_release(dk_op *op)
 {
@@ -152,13 +212,14 @@ void op_release(dk_op *op)
 
 /* ---- states ------------------------------------------------------------- */
 
-dk_state *state_alloc(unsigned n, int prec)
+dk_state *state_alloc(unsigned n, int prec, int slot)
 {
 	dk_state *s = (dk_state *)calloc(1, sizeof(dk_state));
 	if (!s)
 		return nullptr;
 	s->n = n;
 	s->prec = prec;
+	s->slot = slot;
 	return s;
 }
 
@@ -238,7 +299,7 @@ int flush(dk_state *s)
 				off += 16 * gt->dim * gt->dim;
 			}
 		cudaError_t e = cudaMemcpyAsync(dblob, host.data(), host.size(),
-						cudaMemcpyHostToDevice, g.st);
+						cudaMemcpyHostToDevice, CUR.st);
 		if (e != cudaSuccess) {
 			dev_free(dblob, blob_al + gen_bytes);
 			dk_plan_free(&plan);
@@ -268,7 +329,7 @@ int flush(dk_state *s)
 			const dk_sweep_hdr *hp =
 				(const dk_sweep_hdr *)(plan.blob + stp.prog_off);
 			e = dk::launch_sweep(prec, cur, dst->d, dblob + stp.prog_off, hp,
-					     cur_sc, dst->sc, g.scratch, g.num_sms, g.st);
+					     cur_sc, dst->sc, CUR.scratch, g.num_sms, CUR.st);
 			g.sweeps++;
 			g.gates += (unsigned long long)stp.ngates;
 		} else {
@@ -284,7 +345,7 @@ int flush(dk_state *s)
 			e = dk::launch_generic_gate(prec, cur, target, n, op.k, op.tg,
 						    op.cm, op.am,
 						    (const double *)(dblob + gen_off[i]),
-						    cur_sc, dst->sc, g.scratch, g.st);
+						    cur_sc, dst->sc, CUR.scratch, CUR.st);
 			if (tmp) {
 				dev_free(dst->d, dst->bytes);
 				dst->d = tmp;
@@ -318,9 +379,9 @@ int read_scal(dk_state *s)
 	if (s->have_norm)
 		return DK_OK;
 	dk_scal sc;
-	CK(cudaMemcpyAsync(&sc, s->buf->sc, sizeof(sc), cudaMemcpyDeviceToHost, g.st));
+	CK(cudaMemcpyAsync(&sc, s->buf->sc, sizeof(sc), cudaMemcpyDeviceToHost, CUR.st));
 	g.d2h += sizeof(sc);
-	CK(cudaStreamSynchronize(g.st));
+	CK(cudaStreamSynchronize(CUR.st));
 	s->norm = sc.norm;
 	s->csq = sc.csq;
 	s->have_norm = 1;
@@ -356,12 +417,12 @@ int fill_hcache(dk_state *s)
 		free(h);
 		return rc;
 	}
-	cudaError_t e = dk::launch_export(s->prec, s->buf->d, 0, size, tmp, g.st);
+	cudaError_t e = dk::launch_export(s->prec, s->buf->d, 0, size, tmp, CUR.st);
 	if (e == cudaSuccess)
-		e = cudaMemcpyAsync(h, tmp, 16 * size, cudaMemcpyDeviceToHost, g.st);
+		e = cudaMemcpyAsync(h, tmp, 16 * size, cudaMemcpyDeviceToHost, CUR.st);
 	g.d2h += 16 * size;
 	if (e == cudaSuccess)
-		e = cudaStreamSynchronize(g.st);
+		e = cudaStreamSynchronize(CUR.st);
 	dev_free(tmp, 16 * size);
 	if (e != cudaSuccess) {
 		free(h);
@@ -376,11 +437,11 @@ int fill_hcache(dk_state *s)
 int marginals_to_scratch(dk_state *s)
 {
 	if (s->have_marg) {
-		CK(cudaMemcpyAsync(g.scratch.marg, s->marg, sizeof(double) * (s->n + 1),
-				   cudaMemcpyHostToDevice, g.st));
+		CK(cudaMemcpyAsync(CUR.scratch.marg, s->marg, sizeof(double) * (s->n + 1),
+				   cudaMemcpyHostToDevice, CUR.st));
 		return DK_OK;
 	}
-	CK(dk::launch_marginals(s->prec, s->buf->d, s->n, g.scratch, g.st));
+	CK(dk::launch_marginals(s->prec, s->buf->d, s->n, CUR.scratch, CUR.st));
 	return DK_OK;
 }
 
@@ -414,8 +475,8 @@ const char *dk_last_cuda_error(void) { return g.err; }
 
 int dk_init(int device)
 {
-	Lock lk;
-	if (g.inited)
+	std::lock_guard<std::mutex> lk(g.init_mu);
+	if (g.inited.load())
 		return DK_OK;
 	int count = 0;
 	if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -426,19 +487,22 @@ int dk_init(int device)
 		const char *env = getenv("DK_DEVICE");
 		device = env ? atoi(env) : 0;
 	}
-	CK(cudaSetDevice(device));
+	cudaError_t e = cudaSetDevice(device);
+	if (e != cudaSuccess)
+		return cuda_fail(e);
 	g.device = device;
-	CK(cudaDeviceGetAttribute(&g.num_sms, cudaDevAttrMultiProcessorCount, device));
-	CK(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+	e = cudaDeviceGetAttribute(&g.num_sms, cudaDevAttrMultiProcessorCount, device);
+	if (e != cudaSuccess)
+		return cuda_fail(e);
 	cudaMemPool_t pool;
 	if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
 		uint64_t thr = UINT64_MAX;
 		cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
 	}
-	CK(cudaMalloc(&g.scratch.partials,
-		      sizeof(double) * dk::kMaxBlocks * dk::kPartialStride));
-	CK(cudaMalloc(&g.scratch.u64, 4 * sizeof(unsigned long long)));
-	CK(cudaMalloc(&g.scratch.marg, 64 * sizeof(double)));
+	int rc = create_slot(0);
+	if (rc)
+		return rc;
+	g.nslots = 1;
 	const char *b = getenv("DK_HBM_BUDGET_BYTES");
 	g.budget = b ? (size_t)strtoull(b, nullptr, 10) : 0;
 	const char *tb = getenv("DK_TILE_BITS");
@@ -450,6 +514,40 @@ int dk_init(int device)
 	g.inited = 1;
 	return DK_OK;
 }
+
+int dk_slot_new(int *slot)
+{
+	if (!slot)
+		return DK_ERR_ARG;
+	int rc = ensure_init();
+	if (rc)
+		return rc;
+	std::lock_guard<std::mutex> lk(g.slots_mu);
+	const int id = g.nslots.load();
+	if (id >= kMaxSlots)
+		return DK_ERR_ARG;
+	cudaSetDevice(g.device);
+	rc = create_slot(id);
+	if (rc)
+		return rc;
+	g.nslots = id + 1;
+	*slot = id;
+	return DK_OK;
+}
+
+int dk_slot_set(int slot)
+{
+	int rc = ensure_init();
+	if (rc)
+		return rc;
+	if (slot < 0 || slot >= g.nslots.load())
+		return DK_ERR_ARG;
+	cudaSetDevice(g.device);
+	t_slot = slot;
+	return DK_OK;
+}
+
+int dk_slot_get(void) { return t_slot; }
 
 int dk_gate_new(unsigned num_qubits, const double *matrix, dk_gate **out)
 {
@@ -485,8 +583,7 @@ void dk_gate_free(dk_gate *gate)
 {
 	if (!gate)
 		return;
-	Lock lk;
-	if (--gate->refcount > 0)
+	if (__atomic_sub_fetch(&gate->refcount, 1, __ATOMIC_ACQ_REL) > 0)
 		return;
 	free(gate->m);
 	free(gate);
@@ -494,7 +591,9 @@ void dk_gate_free(dk_gate *gate)
 
 int dk_state_new(unsigned num_qubits, int precision, dk_state **out)
 {
-	Lock lk;
+	if (ensure_init() != DK_OK)
+		return ensure_init();
+	SlotLock lk(t_slot);
 	if (!out || (precision != DK_C64 && precision != DK_C128))
 		return DK_ERR_ARG;
 	if (num_qubits == 0)
@@ -504,7 +603,7 @@ int dk_state_new(unsigned num_qubits, int precision, dk_state **out)
 	int rc = ensure_init();
 	if (rc)
 		return rc;
-	dk_state *s = state_alloc(num_qubits, precision);
+	dk_state *s = state_alloc(num_qubits, precision, t_slot);
 	if (!s)
 		return DK_ERR_ALLOC;
 	rc = buf_new(num_qubits, precision, &s->buf);
@@ -513,7 +612,7 @@ int dk_state_new(unsigned num_qubits, int precision, dk_state **out)
 		return rc;
 	}
 	cudaError_t e = dk::launch_init_zero(precision, s->buf->d, num_qubits,
-					     s->buf->sc, g.st);
+					     s->buf->sc, CUR.st);
 	if (e != cudaSuccess) {
 		dk_state_free(s);
 		return cuda_fail(e);
@@ -525,7 +624,9 @@ int dk_state_new(unsigned num_qubits, int precision, dk_state **out)
 int dk_state_from_host(unsigned num_qubits, int precision, const double *values,
 		       dk_state **out)
 {
-	Lock lk;
+	if (ensure_init() != DK_OK)
+		return ensure_init();
+	SlotLock lk(t_slot);
 	if (!out || !values || (precision != DK_C64 && precision != DK_C128))
 		return DK_ERR_ARG;
 	if (num_qubits == 0)
@@ -535,7 +636,7 @@ int dk_state_from_host(unsigned num_qubits, int precision, const double *values,
 	int rc = ensure_init();
 	if (rc)
 		return rc;
-	dk_state *s = state_alloc(num_qubits, precision);
+	dk_state *s = state_alloc(num_qubits, precision, t_slot);
 	if (!s)
 		return DK_ERR_ALLOC;
 	rc = buf_new(num_qubits, precision, &s->buf);
@@ -552,13 +653,13 @@ int dk_state_from_host(unsigned num_qubits, int precision, const double *values,
 			return rc;
 		}
 	}
-	cudaError_t e = cudaMemcpyAsync(stage, values, bytes, cudaMemcpyHostToDevice, g.st);
+	cudaError_t e = cudaMemcpyAsync(stage, values, bytes, cudaMemcpyHostToDevice, CUR.st);
 	g.h2d += bytes;
 	if (e == cudaSuccess)
 		e = dk::launch_import(precision, stage, s->buf->d, num_qubits, s->buf->sc,
-				      g.scratch, g.st);
+				      CUR.scratch, CUR.st);
 	if (e == cudaSuccess)
-		e = cudaStreamSynchronize(g.st);
+		e = cudaStreamSynchronize(CUR.st);
 	if (precision == DK_C64)
 		dev_free(stage, bytes);
 	if (e != cudaSuccess) {
@@ -571,13 +672,13 @@ int dk_state_from_host(unsigned num_qubits, int precision, const double *values,
 
 int dk_state_clone(dk_state *src, dk_state **out)
 {
-	Lock lk;
+	SlotLock lk(src ? src->slot : t_slot);
 	int rc = check_live(src);
 	if (rc)
 		return rc;
 	if (!out)
 		return DK_ERR_ARG;
-	dk_state *s = state_alloc(src->n, src->prec);
+	dk_state *s = state_alloc(src->n, src->prec, src->slot);
 	if (!s)
 		return DK_ERR_ALLOC;
 	s->buf = src->buf;
@@ -594,7 +695,7 @@ void dk_state_release(dk_state *s)
 {
 	if (!s)
 		return;
-	Lock lk;
+	SlotLock lk(s->slot);
 	buf_release(s->buf);
 	s->buf = nullptr;
 	op_release(s->pending);
@@ -607,7 +708,7 @@ void dk_state_free(dk_state *s)
 {
 	if (!s)
 		return;
-	Lock lk;
+	SlotLock lk(s->slot);
 	buf_release(s->buf);
 	op_release(s->pending);
 	state_drop_caches(s);
@@ -633,7 +734,7 @@ int dk_apply_gate(dk_state *in, const dk_gate *gate, const unsigned *targets,
 		  unsigned num_controls, const unsigned *anticontrols,
 		  unsigned num_anticontrols, dk_state **out)
 {
-	Lock lk;
+	SlotLock lk(in ? in->slot : t_slot);
 	int rc = check_live(in);
 	if (rc)
 		return rc;
@@ -664,7 +765,7 @@ int dk_apply_gate(dk_state *in, const dk_gate *gate, const unsigned *targets,
 	dk_op *op = (dk_op *)calloc(1, sizeof(dk_op));
 	if (!op)
 		return DK_ERR_ALLOC;
-	dk_state *s = state_alloc(in->n, in->prec);
+	dk_state *s = state_alloc(in->n, in->prec, in->slot);
 	if (!s) {
 		free(op);
 		return DK_ERR_ALLOC;
@@ -690,7 +791,7 @@ int dk_apply_gate(dk_state *in, const dk_gate *gate, const unsigned *targets,
 
 int dk_get_amplitude(dk_state *s, uint64_t id, double *re, double *im)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
 		return rc;
@@ -709,16 +810,16 @@ int dk_get_amplitude(dk_state *s, uint64_t id, double *re, double *im)
 	double v[2];
 	if (s->prec == DK_C128) {
 		CK(cudaMemcpyAsync(v, (const double2 *)s->buf->d + id, 16,
-				   cudaMemcpyDeviceToHost, g.st));
+				   cudaMemcpyDeviceToHost, CUR.st));
 	} else {
 		float f[2];
 		CK(cudaMemcpyAsync(f, (const float2 *)s->buf->d + id, 8,
-				   cudaMemcpyDeviceToHost, g.st));
-		CK(cudaStreamSynchronize(g.st));
+				   cudaMemcpyDeviceToHost, CUR.st));
+		CK(cudaStreamSynchronize(CUR.st));
 		v[0] = f[0];
 		v[1] = f[1];
 	}
-	CK(cudaStreamSynchronize(g.st));
+	CK(cudaStreamSynchronize(CUR.st));
 	*re = v[0] / s->norm;
 	*im = v[1] / s->norm;
 	return DK_OK;
@@ -726,7 +827,7 @@ int dk_get_amplitude(dk_state *s, uint64_t id, double *re, double *im)
 
 int dk_get_amplitudes(dk_state *s, uint64_t first, uint64_t count, double *out)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
 		return rc;
@@ -743,12 +844,12 @@ int dk_get_amplitudes(dk_state *s, uint64_t first, uint64_t count, double *out)
 	rc = dev_alloc((void **)&tmp, 16 * count);
 	if (rc)
 		return rc;
-	cudaError_t e = dk::launch_export(s->prec, s->buf->d, first, count, tmp, g.st);
+	cudaError_t e = dk::launch_export(s->prec, s->buf->d, first, count, tmp, CUR.st);
 	if (e == cudaSuccess)
-		e = cudaMemcpyAsync(out, tmp, 16 * count, cudaMemcpyDeviceToHost, g.st);
+		e = cudaMemcpyAsync(out, tmp, 16 * count, cudaMemcpyDeviceToHost, CUR.st);
 	g.d2h += 16 * count;
 	if (e == cudaSuccess)
-		e = cudaStreamSynchronize(g.st);
+		e = cudaStreamSynchronize(CUR.st);
 	dev_free(tmp, 16 * count);
 	if (e != cudaSuccess)
 		return cuda_fail(e);
@@ -759,7 +860,7 @@ int dk_get_amplitudes(dk_state *s, uint64_t first, uint64_t count, double *out)
 
 int dk_global_phase(dk_state *s, double *phase)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
 		return rc;
@@ -773,11 +874,11 @@ int dk_global_phase(dk_state *s, double *phase)
 	uint64_t first = 0, chunk = 1ull << 16, found = UINT64_MAX;
 	while (first < size) {
 		const uint64_t cnt = chunk < size - first ? chunk : size - first;
-		CK(dk::launch_first_nonzero(s->prec, s->buf->d, first, cnt, g.scratch,
-					    g.st));
+		CK(dk::launch_first_nonzero(s->prec, s->buf->d, first, cnt, CUR.scratch,
+					    CUR.st));
 		unsigned long long hv = 0;
-		CK(cudaMemcpyAsync(&hv, g.scratch.u64, 8, cudaMemcpyDeviceToHost, g.st));
-		CK(cudaStreamSynchronize(g.st));
+		CK(cudaMemcpyAsync(&hv, CUR.scratch.u64, 8, cudaMemcpyDeviceToHost, CUR.st));
+		CK(cudaStreamSynchronize(CUR.st));
 		if (hv != ~0ull) {
 			found = hv;
 			break;
@@ -802,7 +903,7 @@ int dk_global_phase(dk_state *s, double *phase)
 
 int dk_marginals(dk_state *s, double *p)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
 		return rc;
@@ -812,13 +913,13 @@ int dk_marginals(dk_state *s, double *p)
 		double *m = (double *)malloc(sizeof(double) * (s->n + 1));
 		if (!m)
 			return DK_ERR_ALLOC;
-		cudaError_t e = dk::launch_marginals(s->prec, s->buf->d, s->n, g.scratch, g.st);
+		cudaError_t e = dk::launch_marginals(s->prec, s->buf->d, s->n, CUR.scratch, CUR.st);
 		if (e == cudaSuccess)
-			e = cudaMemcpyAsync(m, g.scratch.marg, sizeof(double) * (s->n + 1),
-					    cudaMemcpyDeviceToHost, g.st);
+			e = cudaMemcpyAsync(m, CUR.scratch.marg, sizeof(double) * (s->n + 1),
+					    cudaMemcpyDeviceToHost, CUR.st);
 		g.d2h += sizeof(double) * (s->n + 1);
 		if (e == cudaSuccess)
-			e = cudaStreamSynchronize(g.st);
+			e = cudaStreamSynchronize(CUR.st);
 		if (e != cudaSuccess) {
 			free(m);
 			return cuda_fail(e);
@@ -834,7 +935,7 @@ int dk_marginals(dk_state *s, double *p)
 
 int dk_probability(dk_state *s, unsigned target, double *p)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = check_live(s);
 	if (rc)
 		return rc;
@@ -851,7 +952,7 @@ int dk_probability(dk_state *s, unsigned target, double *p)
 int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 		    unsigned num_rolls, int8_t *results, dk_state **out)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
 		return rc;
@@ -893,11 +994,11 @@ int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 					break;
 			}
 			e = dk::launch_measure_collapse(cur->prec, cur->d, nullptr, 1, q, roll,
-							-1, cur->sc, scratch_sc, g.scratch,
-							g.st);
+							-1, cur->sc, scratch_sc, CUR.scratch,
+							CUR.st);
 			if (e == cudaSuccess)
 				e = cudaMemcpyAsync(&flags[i], &scratch_sc->flag, 4,
-						    cudaMemcpyDeviceToHost, g.st);
+						    cudaMemcpyDeviceToHost, CUR.st);
 			g.d2h += 4;
 			if (e != cudaSuccess)
 				rc = cuda_fail(e);
@@ -913,13 +1014,13 @@ int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 		if (rc)
 			break;
 		e = dk::launch_measure_collapse(cur->prec, cur->d, nb->d, cur_n, q, roll,
-						-1, cur->sc, nb->sc, g.scratch, g.st);
+						-1, cur->sc, nb->sc, CUR.scratch, CUR.st);
 		if (e == cudaSuccess)
 			e = cudaMemcpyAsync(&flags[i], &nb->sc->flag, 4,
-					    cudaMemcpyDeviceToHost, g.st);
+					    cudaMemcpyDeviceToHost, CUR.st);
 		g.d2h += 4;
 		if (e == cudaSuccess && left > 0)
-			e = dk::launch_marginals(nb->prec, nb->d, cur_n - 1, g.scratch, g.st);
+			e = dk::launch_marginals(nb->prec, nb->d, cur_n - 1, CUR.scratch, CUR.st);
 		if (e != cudaSuccess) {
 			rc = cuda_fail(e);
 			buf_release(nb);
@@ -931,7 +1032,7 @@ int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 		cur = nb;
 		cur_n--;
 	}
-	cudaError_t e = cudaStreamSynchronize(g.st);
+	cudaError_t e = cudaStreamSynchronize(CUR.st);
 	if (scratch_sc)
 		dev_free(scratch_sc, sizeof(dk_scal));
 	if (rc == DK_OK && e != cudaSuccess)
@@ -958,7 +1059,7 @@ int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 		*out = nullptr;
 		return DK_OK;
 	}
-	dk_state *ns = state_alloc(cur_n, s->prec);
+	dk_state *ns = state_alloc(cur_n, s->prec, s->slot);
 	if (!ns) {
 		buf_release(owned);
 		return DK_ERR_ALLOC;
@@ -971,7 +1072,7 @@ int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 int dk_measure(dk_state *s, unsigned target, double roll, int *result,
 	       dk_state **out)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = check_live(s);
 	if (rc)
 		return rc;
@@ -987,11 +1088,32 @@ int dk_measure(dk_state *s, unsigned target, double roll, int *result,
 
 int dk_join(dk_state *most, dk_state *least, dk_state **out)
 {
-	Lock lk;
-	int rc = prepare_read(most);
-	if (rc)
-		return rc;
-	rc = prepare_read(least);
+	if (!most || !least)
+		return DK_ERR_ARG;
+	int rc;
+	cudaEvent_t ready = nullptr;
+	if (least->slot != most->slot) {
+		/* the least register is flushed on its own slot; most's slot waits */
+		SlotLock lk2(least->slot);
+		rc = prepare_read(least);
+		if (rc)
+			return rc;
+		if (cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess ||
+		    cudaEventRecord(ready, CUR.st) != cudaSuccess) {
+			if (ready)
+				cudaEventDestroy(ready);
+			return cuda_fail(cudaGetLastError());
+		}
+	}
+	SlotLock lk(most->slot);
+	rc = prepare_read(most);
+	if (rc == DK_OK && !ready)
+		rc = prepare_read(least);
+	if (ready) {
+		if (rc == DK_OK && cudaStreamWaitEvent(CUR.st, ready, 0) != cudaSuccess)
+			rc = cuda_fail(cudaGetLastError());
+		cudaEventDestroy(ready);
+	}
 	if (rc)
 		return rc;
 	if (!out || most->prec != least->prec)
@@ -999,7 +1121,7 @@ int dk_join(dk_state *most, dk_state *least, dk_state **out)
 	const unsigned n = most->n + least->n;
 	if (n > DK_MAX_QUBITS)
 		return DK_ERR_QUBITS;
-	dk_state *s = state_alloc(n, most->prec);
+	dk_state *s = state_alloc(n, most->prec, most->slot);
 	if (!s)
 		return DK_ERR_ALLOC;
 	rc = buf_new(n, most->prec, &s->buf);
@@ -1009,7 +1131,7 @@ int dk_join(dk_state *most, dk_state *least, dk_state **out)
 	}
 	cudaError_t e = dk::launch_join(most->prec, most->buf->d, most->n, most->buf->sc,
 					least->buf->d, least->n, least->buf->sc,
-					s->buf->d, s->buf->sc, g.scratch, g.st);
+					s->buf->d, s->buf->sc, CUR.scratch, CUR.st);
 	if (e != cudaSuccess) {
 		dk_state_free(s);
 		return cuda_fail(e);
@@ -1020,7 +1142,7 @@ int dk_join(dk_state *most, dk_state *least, dk_state **out)
 
 int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
 		return rc;
@@ -1033,12 +1155,12 @@ int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)
 		return DK_ERR_ARG;
 	const uint64_t dim = 1ull << k;
 	const uint64_t K = 1ull << (n - k);
-	if (!g.blas) {
-		if (cublasCreate(&g.blas) != CUBLAS_STATUS_SUCCESS) {
+	if (!CUR.blas) {
+		if (cublasCreate(&CUR.blas) != CUBLAS_STATUS_SUCCESS) {
 			snprintf(g.err, sizeof(g.err), "cublasCreate failed");
 			return DK_ERR_CUDA;
 		}
-		cublasSetStream(g.blas, g.st);
+		cublasSetStream(CUR.blas, CUR.st);
 	}
 	const bool direct = (s->prec == DK_C128) && (keep_mask == dim - 1);
 	double2 *C = nullptr, *rho = nullptr, *M = nullptr;
@@ -1061,7 +1183,7 @@ int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)
 	cudaError_t e = cudaSuccess;
 	const double2 *A = (const double2 *)s->buf->d;
 	if (!direct) {
-		e = dk::launch_gather_kept(s->prec, s->buf->d, n, keep_mask, M, g.st);
+		e = dk::launch_gather_kept(s->prec, s->buf->d, n, keep_mask, M, CUR.st);
 		A = M;
 	}
 	const double alpha = 1.0 / (s->norm * s->norm);
@@ -1071,18 +1193,18 @@ int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)
 	     k0 += chunk) {
 		const uint64_t kc = (K - k0) < chunk ? (K - k0) : chunk;
 		const double beta = k0 ? 1.0 : 0.0;
-		bs = cublasZherk(g.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, (int)dim,
+		bs = cublasZherk(CUR.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, (int)dim,
 				 (int)kc, &alpha,
 				 (const cuDoubleComplex *)(A + k0 * dim), (int)dim, &beta,
 				 (cuDoubleComplex *)C, (int)dim);
 	}
 	if (e == cudaSuccess && bs == CUBLAS_STATUS_SUCCESS)
-		e = dk::launch_herm_fill(C, rho, dim, g.st);
+		e = dk::launch_herm_fill(C, rho, dim, CUR.st);
 	if (e == cudaSuccess && bs == CUBLAS_STATUS_SUCCESS)
-		e = cudaMemcpyAsync(out, rho, 16 * dim * dim, cudaMemcpyDeviceToHost, g.st);
+		e = cudaMemcpyAsync(out, rho, 16 * dim * dim, cudaMemcpyDeviceToHost, CUR.st);
 	g.d2h += 16 * dim * dim;
 	if (e == cudaSuccess)
-		e = cudaStreamSynchronize(g.st);
+		e = cudaStreamSynchronize(CUR.st);
 	dev_free(C, 16 * dim * dim);
 	dev_free(rho, 16 * dim * dim);
 	if (M)
@@ -1099,7 +1221,7 @@ int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)
 int dk_reduced_density_elem(dk_state *s, uint64_t keep_mask, uint64_t i,
 			    uint64_t j, double *re, double *im)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
 		return rc;
@@ -1110,9 +1232,9 @@ int dk_reduced_density_elem(dk_state *s, uint64_t keep_mask, uint64_t i,
 		return DK_ERR_ARG;
 	double v[2];
 	CK(dk::launch_rho_elem(s->prec, s->buf->d, n, keep_mask, i, j, s->buf->sc,
-			       g.scratch, g.st));
-	CK(cudaMemcpyAsync(v, g.scratch.marg, 16, cudaMemcpyDeviceToHost, g.st));
-	CK(cudaStreamSynchronize(g.st));
+			       CUR.scratch, CUR.st));
+	CK(cudaMemcpyAsync(v, CUR.scratch.marg, 16, cudaMemcpyDeviceToHost, CUR.st));
+	CK(cudaStreamSynchronize(CUR.st));
 	*re = v[0];
 	*im = v[1];
 	return DK_OK;
@@ -1120,14 +1242,14 @@ int dk_reduced_density_elem(dk_state *s, uint64_t keep_mask, uint64_t i,
 
 int dk_set_fusion(int enable)
 {
-	Lock lk;
+	
 	g.fuse = enable ? 1 : 0;
 	return DK_OK;
 }
 
 int dk_get_stats(uint64_t *kernel_launches, uint64_t *sweeps, uint64_t *gates_applied)
 {
-	Lock lk;
+	
 	if (kernel_launches)
 		*kernel_launches = dk::g_launches;
 	if (sweeps)
@@ -1139,7 +1261,7 @@ int dk_get_stats(uint64_t *kernel_launches, uint64_t *sweeps, uint64_t *gates_ap
 
 int dk_get_io_stats(uint64_t *h2d_bytes, uint64_t *d2h_bytes)
 {
-	Lock lk;
+	
 	if (h2d_bytes)
 		*h2d_bytes = g.h2d;
 	if (d2h_bytes)
@@ -1149,7 +1271,7 @@ int dk_get_io_stats(uint64_t *h2d_bytes, uint64_t *d2h_bytes)
 
 int dk_state_flush(dk_state *s)
 {
-	Lock lk;
+	SlotLock lk(s ? s->slot : t_slot);
 	int rc = check_live(s);
 	if (rc)
 		return rc;
@@ -1161,14 +1283,23 @@ int dk_state_flush(dk_state *s)
 	return flush(s);
 }
 
-void *dk_stream(void) { return (void *)g.st; }
+void *dk_stream(void)
+{
+	if (!g.inited.load())
+		return nullptr;
+	Slot *sl = g.slots[t_slot];
+	return sl ? (void *)sl->st : nullptr;
+}
 
 int dk_sync(void)
 {
-	Lock lk;
-	if (!g.inited)
+	if (!g.inited.load())
 		return DK_OK;
-	CK(cudaStreamSynchronize(g.st));
+	const int ns = g.nslots.load();
+	for (int i = 0; i < ns; ++i) {
+		SlotLock lk(i);
+		CK(cudaStreamSynchronize(CUR.st));
+	}
 	return DK_OK;
 }
 

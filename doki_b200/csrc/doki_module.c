@@ -17,7 +17,8 @@
  *   registry_probs(reg) -> list of all P(q = 1);
  *   funmatrix_numpy(fm) -> numpy array of a density / reduced density matrix;
  *   registry_precision(reg); registry_flush(reg); engine_sync();
- *   engine_set_fusion(bool); engine_stats(); engine_stream().
+ *   engine_set_fusion(bool); engine_stats(); engine_stream();
+ *   engine_new_slot(); engine_set_slot(slot); engine_get_slot().
  */
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>
@@ -1034,6 +1035,30 @@ static PyObject *doki_engine_stats(PyObject *self, PyObject *args)
 			     "d2h_bytes", (unsigned long long)ho);
 }
 
+static PyObject *doki_engine_new_slot(PyObject *self, PyObject *args)
+{
+	int slot = -1, rc;
+	Py_BEGIN_ALLOW_THREADS rc = dk_slot_new(&slot);
+	Py_END_ALLOW_THREADS if (rc) return raise_dk(rc, "Failed to create a stream slot");
+	return PyLong_FromLong(slot);
+}
+
+static PyObject *doki_engine_set_slot(PyObject *self, PyObject *args)
+{
+	int slot;
+	if (!PyArg_ParseTuple(args, "i", &slot))
+		return NULL;
+	int rc = dk_slot_set(slot);
+	if (rc)
+		return raise_dk(rc, "Failed to select the stream slot");
+	Py_RETURN_NONE;
+}
+
+static PyObject *doki_engine_get_slot(PyObject *self, PyObject *args)
+{
+	return PyLong_FromLong(dk_slot_get());
+}
+
 static PyObject *doki_engine_stream(PyObject *self, PyObject *args)
 {
 	return PyLong_FromVoidPtr(dk_stream());
@@ -1462,6 +1487,12 @@ static PyMethodDef DokiMethods[] = {
 	  "Enable (default) or disable multi-gate sweep fusion" },
 	{ "engine_stats", doki_engine_stats, METH_VARARGS,
 	  "Kernel launches, sweeps, gates and host<->device bytes so far" },
+	{ "engine_new_slot", doki_engine_new_slot, METH_VARARGS,
+	  "Create a stream slot (own CUDA stream and scratch); returns its id" },
+	{ "engine_set_slot", doki_engine_set_slot, METH_VARARGS,
+	  "Select the slot new registries of this thread are created on" },
+	{ "engine_get_slot", doki_engine_get_slot, METH_VARARGS,
+	  "Slot new registries of this thread are created on" },
 	{ "engine_stream", doki_engine_stream, METH_VARARGS,
 	  "Address of the CUDA stream the engine queues its work on" },
 	{ "registry_flush", doki_registry_flush, METH_VARARGS,

@@ -1,0 +1,191 @@
+"""Serving form: continuous batching of circuit requests under an HBM budget.
+
+Requests arrive as a Poisson stream.  Each carries a circuit of n qubits
+(log-uniform in [qmin, qmax]) and depth d (uniform in [dmin, dmax]) drawn
+from the plain method's CPU-runnable generator (U3 on every qubit, CNOT on a
+random pairing, one Toffoli with an anticontrol per layer), and a terminal
+operation: all single-qubit probabilities, or the measurement of k in [1, 8]
+random qubits with seeded draws.
+
+The server keeps `workers` requests in flight, each on its own stream slot of
+the engine (so their kernels overlap on the device), admits the next request
+in arrival order as soon as a slot is free and its register fits in the HBM
+budget, keeps every register resident on the device from its first gate to
+its result, and records per-request latency from arrival to result on the
+host.  `workers=1` with no overlap is the plain one-at-a-time path.
+"""
+from __future__ import annotations
+
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import workloads as W
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float  # seconds after the stream starts
+    n: int
+    depth: int
+    seed: int
+    terminal: str  # "probs" or "measure"
+    mask: int = 0
+    rolls: List[float] = field(default_factory=list)
+
+    def circuit(self) -> W.Circuit:
+        return W.small_circuit(seed=self.seed, n=self.n, depth=self.depth)
+
+    def state_bytes(self, precision: int) -> int:
+        return (16 if precision == 2 else 8) << self.n
+
+
+def request_stream(seed: int = 5, count: int = 20000, qmin: int = 8, qmax: int = 28,
+                   dmin: int = 10, dmax: int = 100, rate: float = 1.0) -> List[Request]:
+    """`count` requests; inter-arrival times ~ Exp(rate) (requests / s)."""
+    rng = W.rng_for(seed)
+    ns = np.floor(np.exp(rng.uniform(np.log(qmin), np.log(qmax + 1), size=count))).astype(int)
+    ns = np.clip(ns, qmin, qmax)
+    depths = rng.integers(dmin, dmax + 1, size=count)
+    gaps = rng.exponential(1.0 / rate, size=count) if rate > 0 else np.zeros(count)
+    arrivals = np.cumsum(gaps) - (gaps[0] if count else 0.0)
+    out = []
+    for i in range(count):
+        n = int(ns[i])
+        if rng.random() < 0.5:
+            out.append(Request(i, float(arrivals[i]), n, int(depths[i]), 10_000 + i, "probs"))
+        else:
+            k = int(rng.integers(1, 9))
+            qs = rng.choice(n, size=min(k, n), replace=False)
+            mask = 0
+            for q in qs:
+                mask |= 1 << int(q)
+            out.append(Request(i, float(arrivals[i]), n, int(depths[i]), 10_000 + i,
+                               "measure", mask, rng.random(len(qs)).tolist()))
+    return out
+
+
+def with_rate(reqs: Sequence[Request], rate: float, seed: int = 6) -> List[Request]:
+    """The same requests re-timed as a Poisson stream of `rate` requests / s."""
+    rng = W.rng_for(seed)
+    gaps = rng.exponential(1.0 / rate, size=len(reqs))
+    arr = np.cumsum(gaps) - gaps[0]
+    return [Request(r.rid, float(a), r.n, r.depth, r.seed, r.terminal, r.mask, r.rolls)
+            for r, a in zip(reqs, arr)]
+
+
+def execute(d, req: Request, precision: int):
+    """Run one request through the doki API on the calling thread's slot."""
+    c = req.circuit()
+    reg = W.run_ops(d, d.registry_new(req.n, False, precision), c.ops)
+    if req.terminal == "probs":
+        return ("probs", d.registry_probs(reg))
+    _, res = d.registry_measure(reg, req.mask, req.rolls, -1, False)
+    return ("measure", res)
+
+
+class Server:
+    """Continuous batching over `workers` engine slots under an HBM budget."""
+
+    def __init__(self, d, workers: int = 8, budget_bytes: float = 150e9, precision: int = 1,
+                 deadline_s: float = 600.0):
+        self.d = d
+        self.workers = workers
+        self.budget = budget_bytes
+        self.precision = precision
+        self.deadline_s = deadline_s
+        self.slots = [0] + [d.engine_new_slot() for _ in range(workers - 1)]
+
+    def run(self, reqs: Sequence[Request], keep_results: bool = False) -> Dict:
+        reqs = sorted(reqs, key=lambda r: r.arrival)
+        lock = threading.Condition()
+        state = {"mem": 0, "free": list(range(self.workers)), "next": 0, "done": 0}
+        queues: List[List[Request]] = [[] for _ in range(self.workers)]
+        latency = np.zeros(len(reqs))
+        finish = np.zeros(len(reqs))
+        results: Dict[int, object] = {}
+        errors: List[BaseException] = []
+        t0 = time.perf_counter()
+        index = {r.rid: i for i, r in enumerate(reqs)}
+
+        def worker(w: int):
+            try:
+                self.d.engine_set_slot(self.slots[w])
+            except BaseException as e:  # noqa: BLE001
+                errors.append(e)
+            while True:
+                with lock:
+                    while not queues[w]:
+                        lock.wait(timeout=1.0)
+                    req = queues[w].pop(0)
+                if req is None:
+                    return
+                res = None
+                if not errors:
+                    try:
+                        res = execute(self.d, req, self.precision)
+                    except BaseException as e:  # noqa: BLE001
+                        errors.append(e)
+                now = time.perf_counter() - t0
+                i = index[req.rid]
+                finish[i] = now
+                latency[i] = now - req.arrival
+                if keep_results:
+                    results[req.rid] = res
+                with lock:
+                    state["mem"] -= 2 * req.state_bytes(self.precision)
+                    state["free"].append(w)
+                    state["done"] += 1
+                    lock.notify_all()
+
+        threads = [threading.Thread(target=worker, args=(w,), daemon=True)
+                   for w in range(self.workers)]
+        for t in threads:
+            t.start()
+        def check():
+            if errors:
+                raise RuntimeError(f"serving worker failed: {errors[0]!r}") from errors[0]
+            if time.perf_counter() - t0 > self.deadline_s:
+                raise TimeoutError(f"serving run exceeded {self.deadline_s} s")
+
+        try:
+            for req in reqs:
+                wait = req.arrival - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+                need = 2 * req.state_bytes(self.precision)
+                with lock:
+                    while not state["free"] or (state["mem"] + need > self.budget
+                                                and state["mem"] > 0):
+                        lock.wait(timeout=1.0)
+                        check()
+                    w = state["free"].pop(0)
+                    state["mem"] += need
+                    queues[w].append(req)
+                    lock.notify_all()
+            with lock:
+                while state["done"] < len(reqs):
+                    lock.wait(timeout=1.0)
+                    check()
+        finally:
+            with lock:
+                for w in range(self.workers):
+                    queues[w].append(None)
+                lock.notify_all()
+            for t in threads:
+                t.join(timeout=60.0)
+        check()
+        makespan = float(finish.max()) if len(reqs) else 0.0
+        return {
+            "requests": len(reqs),
+            "throughput_rps": len(reqs) / makespan if makespan > 0 else 0.0,
+            "p50_ms": float(np.percentile(latency, 50) * 1e3),
+            "p99_ms": float(np.percentile(latency, 99) * 1e3),
+            "mean_ms": float(latency.mean() * 1e3),
+            "makespan_s": makespan,
+            "results": results if keep_results else None,
+        }

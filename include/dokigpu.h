@@ -154,9 +154,19 @@ int dk_get_stats(uint64_t *kernel_launches, uint64_t *sweeps,
 int dk_get_io_stats(uint64_t *h2d_bytes, uint64_t *d2h_bytes);
 /* Execute the gates queued on `s` now (normally deferred to the next read). */
 int dk_state_flush(dk_state *s);
-/* The CUDA stream (cudaStream_t) all of this library's work is queued on,
- * for callers that time it with events; NULL before initialisation. */
+/* The CUDA stream (cudaStream_t) of the calling thread's slot, for callers
+ * that time its work with events; NULL before initialisation. */
 void *dk_stream(void);
+
+/* ---- slots: concurrent streams (no counterpart in the reference) --------
+ * A slot is a CUDA stream with its own scratch.  Registers are created on the
+ * calling thread's current slot (0 unless dk_slot_set was called) and every
+ * register derived from one stays on its slot; work of different slots runs
+ * concurrently on the device and each slot has its own lock, so threads that
+ * drive different slots do not wait for each other.  Up to 64 slots. */
+int dk_slot_new(int *slot);
+int dk_slot_set(int slot);
+int dk_slot_get(void);
 
 /* ---- batching form (no counterpart in the reference) --------------------
  * Thousands of independent registers (4..16 qubits), each starting in |0..0>

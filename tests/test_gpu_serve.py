@@ -1,0 +1,76 @@
+"""Serving form on the GPU: requests served concurrently on several stream
+slots must give the same results as each request run alone, and registers of
+different slots must stay independent (including a join across slots)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from doki_b200 import serve as S
+from doki_b200 import workloads as W
+from tests.conftest import ATOL_C128
+
+pytestmark = pytest.mark.gpu
+
+
+def compare(a, b, atol):
+    assert a[0] == b[0]
+    if a[0] == "probs":
+        assert np.allclose(a[1], b[1], atol=atol, rtol=0)
+    else:
+        assert a[1] == b[1]
+
+
+@pytest.mark.parametrize("precision", [2, 1])
+def test_served_equals_alone(dk_gpu, precision):
+    d = dk_gpu
+    reqs = S.request_stream(seed=33, count=40, qmin=6, qmax=16, dmin=2, dmax=8, rate=400.0)
+    srv = S.Server(d, workers=6, budget_bytes=2e9, precision=precision)
+    mix = srv.run(reqs, keep_results=True)
+    assert mix["requests"] == 40 and mix["p99_ms"] >= mix["p50_ms"] > 0
+    atol = ATOL_C128 if precision == 2 else 1e-6
+    for r in reqs:
+        alone = S.execute(d, r, precision)
+        compare(mix["results"][r.rid], alone, atol)
+
+
+def test_served_matches_oracle(dk_gpu, orc):
+    d = dk_gpu
+    reqs = S.request_stream(seed=34, count=12, qmin=5, qmax=12, dmin=2, dmax=6, rate=1000.0)
+    srv = S.Server(d, workers=4, budget_bytes=1e9, precision=2)
+    out = srv.run(reqs, keep_results=True)
+    for r in reqs:
+        c = r.circuit()
+        reg = W.run_ops(orc, orc.registry_new(r.n), c.ops)
+        got = out["results"][r.rid]
+        if r.terminal == "probs":
+            assert np.allclose(got[1], orc.registry_probs(reg), atol=ATOL_C128)
+        else:
+            _, res = orc.registry_measure(reg, r.mask, r.rolls)
+            assert got[1] == res
+
+
+def test_budget_limits_concurrency(dk_gpu):
+    """With a budget for one register at a time, requests run one by one."""
+    d = dk_gpu
+    reqs = S.request_stream(seed=35, count=6, qmin=14, qmax=14, dmin=2, dmax=3, rate=1e4)
+    one = 2 * reqs[0].state_bytes(2)
+    srv = S.Server(d, workers=4, budget_bytes=one, precision=2)
+    out = srv.run(reqs)
+    assert out["requests"] == 6
+
+
+def test_join_across_slots(dk_gpu, orc):
+    d = dk_gpu
+    s1 = d.engine_new_slot()
+    s2 = d.engine_new_slot()
+    d.engine_set_slot(s1)
+    a = W.run_ops(d, d.registry_new(6, False), W.small_circuit(seed=40, n=6, depth=3).ops)
+    d.engine_set_slot(s2)
+    b = W.run_ops(d, d.registry_new(5, False), W.small_circuit(seed=41, n=5, depth=3).ops)
+    d.engine_set_slot(0)
+    j = d.registry_join(a, b, 1, False)
+    oa = W.run_ops(orc, orc.registry_new(6), W.small_circuit(seed=40, n=6, depth=3).ops)
+    ob = W.run_ops(orc, orc.registry_new(5), W.small_circuit(seed=41, n=5, depth=3).ops)
+    assert np.allclose(d.registry_get_all(j), orc.registry_get_all(orc.registry_join(oa, ob)),
+                       atol=ATOL_C128)

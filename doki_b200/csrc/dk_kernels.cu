@@ -10,6 +10,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "dk_device.cuh"
 #include "dk_kernels.h"
 
@@ -633,8 +635,21 @@ static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dpr
 	const size_t smem = NBUF * (sizeof(C2) << m) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
 			    (size_t)hp->ncond * sizeof(dk_gate_cond) + sizeof(C2) * (size_t)nmat;
 	auto kern = k_sweep<R, SW, M, MINB, NBUF>;
-	cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-					     (int)smem);
+	/* The limit is a per-function attribute shared by every thread: raise it
+	 * once to the device maximum and never lower it, so concurrent launches
+	 * of different sizes from different streams cannot race on it. */
+	static std::once_flag once;
+	static cudaError_t set_err = cudaSuccess;
+	std::call_once(once, [&] {
+		int dev = 0, maxopt = 0;
+		cudaGetDevice(&dev);
+		set_err = cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+						 dev);
+		if (set_err == cudaSuccess)
+			set_err = cudaFuncSetAttribute(
+				kern, cudaFuncAttributeMaxDynamicSharedMemorySize, maxopt);
+	});
+	cudaError_t e = set_err;
 	if (e != cudaSuccess)
 		return e;
 	uint64_t blocks = hp->ntiles;

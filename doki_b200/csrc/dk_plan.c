@@ -39,7 +39,7 @@ void dk_plan_default_limits(int prec, unsigned n, dk_plan_limits *lim)
 	lim->low_bits = m < 4 ? m : 4;
 	lim->max_gates = 512;
 	lim->max_passes = 512;
-	lim->max_mat = 16384;
+	lim->max_mat = 4096; /* complex entries: <= 64 KiB of a sweep's shared memory */
 	lim->fuse = 1;
 }
 

@@ -645,9 +645,14 @@ static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dpr
 		cudaGetDevice(&dev);
 		set_err = cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin,
 						 dev);
+		cudaFuncAttributes fa;
 		if (set_err == cudaSuccess)
-			set_err = cudaFuncSetAttribute(
-				kern, cudaFuncAttributeMaxDynamicSharedMemorySize, maxopt);
+			set_err = cudaFuncGetAttributes(&fa, kern);
+		/* the opt-in limit covers the kernel's static shared memory too */
+		if (set_err == cudaSuccess)
+			set_err = cudaFuncSetAttribute(kern,
+						       cudaFuncAttributeMaxDynamicSharedMemorySize,
+						       maxopt - (int)fa.sharedSizeBytes);
 	});
 	cudaError_t e = set_err;
 	if (e != cudaSuccess)

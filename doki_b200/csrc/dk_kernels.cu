@@ -606,6 +606,56 @@ __global__ void __launch_bounds__(256)
 
 __global__ void k_copy_scal(const dk_scal *a, dk_scal *b) { *b = *a; }
 
+/* Compare two registers of the same size (any precisions): per block
+ * Re / Im of sum conj(x_i) y_i (scaled amplitudes) and max |x_i - y_i|. */
+template <typename RA, typename RB>
+__global__ void __launch_bounds__(256)
+	k_compare(const typename CT<RA>::T *__restrict__ x, double sx,
+		  const typename CT<RB>::T *__restrict__ y, double sy, uint64_t size,
+		  double *partials)
+{
+	double re = 0.0, im = 0.0, mx = 0.0;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < size;
+	     i += (uint64_t)gridDim.x * blockDim.x) {
+		const double2 a = to_c128(__ldcs(x + i)), b = to_c128(__ldcs(y + i));
+		const double ax = a.x * sx, ay = a.y * sx, bx = b.x * sy, by = b.y * sy;
+		re += ax * bx + ay * by;
+		im += ax * by - ay * bx;
+		const double dx = ax - bx, dy = ay - by;
+		mx = fmax(mx, sqrt(dx * dx + dy * dy));
+	}
+	block_sum2(re, im);
+	__shared__ double red[32];
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+	if ((threadIdx.x & 31) == 0)
+		red[threadIdx.x >> 5] = mx;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (unsigned w = 1; w < (blockDim.x + 31) / 32; ++w)
+			mx = fmax(mx, red[w]);
+		partials[3 * blockIdx.x] = re;
+		partials[3 * blockIdx.x + 1] = im;
+		partials[3 * blockIdx.x + 2] = mx;
+	}
+}
+
+__global__ void k_compare_finalize(const double *partials, int nb, double *out)
+{
+	if (threadIdx.x != 0)
+		return;
+	double re = 0.0, im = 0.0, mx = 0.0;
+	for (int b = 0; b < nb; ++b) {
+		re += partials[3 * b];
+		im += partials[3 * b + 1];
+		mx = fmax(mx, partials[3 * b + 2]);
+	}
+	out[0] = re;
+	out[1] = im;
+	out[2] = mx;
+}
+
 inline int grid_for(uint64_t work, int per_block, int cap)
 {
 	uint64_t b = (work + per_block - 1) / per_block;
@@ -951,6 +1001,32 @@ cudaError_t launch_export(int prec, const void *d, uint64_t first, uint64_t coun
 		k_export<float><<<blocks, 256, 0, st>>>((const float2 *)d, first, count,
 						       dst);
 	g_launches += 1;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_compare(int prec_x, const void *x, double sx, int prec_y, const void *y,
+			   double sy, unsigned n, const Scratch &s, cudaStream_t st)
+{
+	const uint64_t size = 1ull << n;
+	const int blocks = grid_for(size, 256 * 4, g_num_sms * 8);
+	if (prec_x == DK_C128 && prec_y == DK_C128)
+		k_compare<double, double><<<blocks, 256, 0, st>>>((const double2 *)x, sx,
+								  (const double2 *)y, sy, size,
+								  s.partials);
+	else if (prec_x == DK_C64 && prec_y == DK_C128)
+		k_compare<float, double><<<blocks, 256, 0, st>>>((const float2 *)x, sx,
+								 (const double2 *)y, sy, size,
+								 s.partials);
+	else if (prec_x == DK_C128 && prec_y == DK_C64)
+		k_compare<double, float><<<blocks, 256, 0, st>>>((const double2 *)x, sx,
+								 (const float2 *)y, sy, size,
+								 s.partials);
+	else
+		k_compare<float, float><<<blocks, 256, 0, st>>>((const float2 *)x, sx,
+								(const float2 *)y, sy, size,
+								s.partials);
+	k_compare_finalize<<<1, 32, 0, st>>>(s.partials, blocks, s.marg);
+	g_launches += 2;
 	return cudaGetLastError();
 }
 

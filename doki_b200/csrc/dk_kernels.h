@@ -92,6 +92,11 @@ cudaError_t launch_rho_elem(int prec, const void *d, unsigned n,
 cudaError_t launch_export(int prec, const void *d, uint64_t first,
 			  uint64_t count, double2 *dst, cudaStream_t st);
 
+/* fidelity terms of two registers: s.marg[0..2] = Re, Im of sum conj(sx x)
+ * (sy y) and max |sx x - sy y| */
+cudaError_t launch_compare(int prec_x, const void *x, double sx, int prec_y, const void *y,
+			   double sy, unsigned n, const Scratch &s, cudaStream_t st);
+
 /* D2D copy of a register (clone that must diverge), scalars included */
 cudaError_t launch_copy(int prec, const void *src, void *dst, unsigned n,
 			const dk_scal *sc_in, dk_scal *sc_out,

@@ -1240,6 +1240,36 @@ int dk_reduced_density_elem(dk_state *s, uint64_t keep_mask, uint64_t i,
 	return DK_OK;
 }
 
+int dk_compare_states(dk_state *x, dk_state *y, double *fidelity, double *max_amp_err)
+{
+	if (!x || !y || x->n != y->n)
+		return DK_ERR_ARG;
+	if (x->slot != y->slot) {
+		/* bring y up to date on its own slot first */
+		SlotLock lk2(y->slot);
+		int rc = prepare_read(y);
+		if (rc)
+			return rc;
+		CK(cudaStreamSynchronize(CUR.st));
+	}
+	SlotLock lk(x->slot);
+	int rc = prepare_read(x);
+	if (rc == DK_OK)
+		rc = prepare_read(y);
+	if (rc)
+		return rc;
+	double v[3];
+	CK(dk::launch_compare(x->prec, x->buf->d, 1.0 / x->norm, y->prec, y->buf->d, 1.0 / y->norm,
+			      x->n, CUR.scratch, CUR.st));
+	CK(cudaMemcpyAsync(v, CUR.scratch.marg, sizeof(v), cudaMemcpyDeviceToHost, CUR.st));
+	CK(cudaStreamSynchronize(CUR.st));
+	if (fidelity)
+		*fidelity = v[0] * v[0] + v[1] * v[1];
+	if (max_amp_err)
+		*max_amp_err = v[2];
+	return DK_OK;
+}
+
 int dk_set_fusion(int enable)
 {
 	

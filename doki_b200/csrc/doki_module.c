@@ -16,7 +16,8 @@
  *   registry_get_all(reg, canonical) -> numpy complex128 array;
  *   registry_probs(reg) -> list of all P(q = 1);
  *   funmatrix_numpy(fm) -> numpy array of a density / reduced density matrix;
- *   registry_precision(reg); registry_flush(reg); engine_sync();
+ *   registry_precision(reg); registry_flush(reg); registry_compare(a, b);
+ *   engine_sync();
  *   engine_set_fusion(bool); engine_stats(); engine_stream();
  *   engine_new_slot(); engine_set_slot(slot); engine_get_slot().
  */
@@ -1035,6 +1036,26 @@ static PyObject *doki_engine_stats(PyObject *self, PyObject *args)
 			     "d2h_bytes", (unsigned long long)ho);
 }
 
+static PyObject *doki_registry_compare(PyObject *self, PyObject *args)
+{
+	PyObject *c1, *c2;
+	if (!PyArg_ParseTuple(args, "OO", &c1, &c2)) {
+		PyErr_SetString(DokiError, "Syntax: registry_compare(registry1, registry2)");
+		return NULL;
+	}
+	dk_state *a = get_state(c1, "NULL pointer to registry1");
+	if (!a)
+		return NULL;
+	dk_state *b = get_state(c2, "NULL pointer to registry2");
+	if (!b)
+		return NULL;
+	double fid = 0.0, err = 0.0;
+	int rc;
+	Py_BEGIN_ALLOW_THREADS rc = dk_compare_states(a, b, &fid, &err);
+	Py_END_ALLOW_THREADS if (rc) return raise_dk(rc, "Failed to compare registries");
+	return Py_BuildValue("(dd)", fid, err);
+}
+
 static PyObject *doki_engine_new_slot(PyObject *self, PyObject *args)
 {
 	int slot = -1, rc;
@@ -1487,6 +1508,8 @@ static PyMethodDef DokiMethods[] = {
 	  "Enable (default) or disable multi-gate sweep fusion" },
 	{ "engine_stats", doki_engine_stats, METH_VARARGS,
 	  "Kernel launches, sweeps, gates and host<->device bytes so far" },
+	{ "registry_compare", doki_registry_compare, METH_VARARGS,
+	  "(fidelity, max amplitude error) between two registries of equal size" },
 	{ "engine_new_slot", doki_engine_new_slot, METH_VARARGS,
 	  "Create a stream slot (own CUDA stream and scratch); returns its id" },
 	{ "engine_set_slot", doki_engine_set_slot, METH_VARARGS,

@@ -139,6 +139,11 @@ int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out);
 int dk_reduced_density_elem(dk_state *s, uint64_t keep_mask, uint64_t i,
 			    uint64_t j, double *re, double *im);
 
+/* Precision form (no counterpart in the reference): fidelity
+ * |<x|y>|^2 of the two logical (normalised) registers and the largest
+ * |x_i - y_i|, accumulated in FP64; x and y may have different precisions. */
+int dk_compare_states(dk_state *x, dk_state *y, double *fidelity, double *max_amp_err);
+
 /* Wait for all queued device work of this library. */
 int dk_sync(void);
 

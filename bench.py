@@ -47,6 +47,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fusion", action="store_true",
                    help="one sweep per gate (the per-gate plain method)")
+    p.add_argument("--no-forms", action="store_true",
+                   help="skip the batching / serving / precision forms")
+    p.add_argument("--serve-requests", type=int, default=120)
     return p.parse_args()
 
 
@@ -271,12 +274,125 @@ def engine_arm(args, rank, world, local_rank):
         "clocks": clk,
         "fusion": not args.no_fusion,
     }
+    if rank == 0 and world == 1 and not args.no_forms:
+        out["forms"] = run_forms(d, args, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(n, c)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+# ------------------------------------------------------------------- forms --
+
+def plain_circuits_per_s(d, fb, per_size=2):
+    """The plain method (one circuit at a time through the doki API,
+    complex128) on a stratified sample of the batch, weighted to the mix."""
+    import numpy as np
+    from doki_b200 import workloads as W
+    times = {}
+    warm = fb.ops(0)
+    W.run_ops(d, d.registry_new(int(fb.num_qubits[0]), False), warm)
+    for n in range(4, 17):
+        idx = [int(c) for c in np.nonzero(fb.num_qubits == n)[0][:per_size]]
+        for c in idx:
+            t0 = time.perf_counter()
+            reg = W.run_ops(d, d.registry_new(n, False), fb.ops(c))
+            rho = d.registry_density(reg, False)
+            for e in range(n - 1, int(fb.keep[c]) - 1, -1):
+                rho = d.funmatrix_partialtrace(rho, e, False)
+            d.funmatrix_numpy(rho)
+            times.setdefault(n, []).append(time.perf_counter() - t0)
+    hist = np.bincount(fb.num_qubits, minlength=17)
+    total = sum(hist[n] * statistics.mean(v) for n, v in times.items())
+    return fb.count / total
+
+
+def batch_form(d, torch):
+    import numpy as np
+    from doki_b200 import batch as B
+    from doki_b200 import workloads as W
+    fb = W.batch_arrays(seed=4, count=4096)
+    dev = torch.cuda.get_device_name()
+    res = {"workload": "4096 registers, n ~ U[4,16], depth ~ U[10,50], U3 + CNOT + "
+                       "controlled-U3, reduced density matrix of the lower half",
+           "gates": int(fb.op_k.size)}
+    for prec, name in ((1, "c64"), (2, "c128")):
+        tune = B.autotune(fb, prec, tile_bits=(11, 12), ctas=(1,), reps=2, device_name=dev)
+        t0 = time.perf_counter()
+        eng = B.BatchEngine(fb, prec, tile_bits=tune["tile_bits"])
+        build_s = time.perf_counter() - t0
+        eng.run()
+        eng.sync()
+        st = torch.cuda.ExternalStream(eng.stream)
+        ms = []
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            eng.run()
+            b.record(st)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        t0 = time.perf_counter()
+        eng.run()
+        rho, _ = eng.rho_all()
+        out_s = time.perf_counter() - t0
+        eng.close()
+        res[name] = {"circuits_per_s": fb.count / (statistics.median(ms) / 1e3),
+                     "batch_ms_p50": float(np.percentile(ms, 50)),
+                     "batch_ms_p99": float(np.percentile(ms, 99)),
+                     "plan_and_upload_s": build_s,
+                     "e2e_circuits_per_s": fb.count / (build_s + out_s),
+                     "rho_bytes": int(rho.nbytes), "tile_bits": tune["tile_bits"],
+                     "autotune_cached": tune["cached"]}
+    plain = plain_circuits_per_s(d, fb)
+    res["plain_gpu_circuits_per_s"] = plain
+    res["speedup_c64_vs_plain"] = res["c64"]["circuits_per_s"] / plain
+    return res
+
+
+def serve_form(d, count):
+    from doki_b200 import serve as S
+    reqs = S.request_stream(seed=5, count=count)
+    sample = (f"first {count} requests of the seeded 20,000-request stream "
+              "(n log-uniform [8,28], depth U[10,100], probabilities or 1-8 measurements)")
+    srv = S.Server(d, workers=8, budget_bytes=150e9, precision=1, deadline_s=240)
+    cap = srv.run(S.with_rate(reqs, 1e9))
+    out = {"sample": sample, "workers": 8, "budget_bytes": 150e9, "precision": "c64",
+           "capacity_rps": cap["throughput_rps"], "loads": {}}
+    for load in (0.5, 0.8, 1.0):
+        r = srv.run(S.with_rate(reqs, load * cap["throughput_rps"]))
+        out["loads"][f"{int(load * 100)}%"] = {k: r[k] for k in
+                                              ("throughput_rps", "p50_ms", "p99_ms")}
+    plain = S.Server(d, workers=1, budget_bytes=150e9, precision=2, deadline_s=400)
+    p = plain.run(S.with_rate(reqs, 1e9))
+    out["plain_gpu_rps"] = p["throughput_rps"]
+    out["speedup_vs_plain"] = cap["throughput_rps"] / p["throughput_rps"]
+    return out
+
+
+def precision_form(d):
+    from doki_b200 import precision as P
+    r = P.run(d, n=32, depth=60, seed=1)
+    return {"workload": "32-qubit register, complex64 (32 GiB) beside complex128 (64 GiB), "
+                        "depth-60 circuit of the 12-qubit generator family",
+            "worst": r["worst"], "c64_layers_per_s": r["c64_layers_per_s"],
+            "c128_layers_per_s": r["c128_layers_per_s"],
+            "fidelity_per_layer": [round(x["fidelity"], 12) for x in r["layers"]]}
+
+
+def run_forms(d, args, torch):
+    forms = {}
+    for name, fn in (("batch", lambda: batch_form(d, torch)),
+                     ("serve", lambda: serve_form(d, args.serve_requests)),
+                     ("precision", lambda: precision_form(d))):
+        try:
+            forms[name] = fn()
+        except Exception as e:  # noqa: BLE001 -- report, keep the headline line
+            forms[name] = {"error": f"{type(e).__name__}: {e}"}
+        d.engine_set_slot(0)
+    return forms
 
 
 # --------------------------------------------------------------- reference --

@@ -368,6 +368,7 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 		const int m = n <= 12 ? (int)n : tile_bits;
 		dk_plan_limits lim = {};
 		lim.tile_bits = m;
+		lim.tensor = -1; /* the batch kernel runs scalar passes */
 		dk_plan_default_limits(precision, n, &lim);
 		lim.tile_bits = m;
 		if (lim.low_bits > m - 3)

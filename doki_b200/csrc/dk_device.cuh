@@ -236,6 +236,29 @@ __device__ __forceinline__ void g_dense2(C2 (&a)[NA], const PassCtx &pc, uint32_
 	}
 }
 
+/* 8x8 matrix on all three register bits: a folded run of gates or a
+ * 3-qubit gate.  Controls, when present, lie outside the pass bits, so they
+ * hold or fail for all 8 amplitudes of the thread at once. */
+template <bool CTL, typename C2>
+__device__ __forceinline__ void g_dense3(C2 (&a)[NA], const PassCtx &pc, uint32_t lc,
+					 uint32_t la, const C2 *mt)
+{
+	if (CTL && !ctl_ok(pc.gb, lc, la))
+		return;
+	C2 y[NA];
+#pragma unroll
+	for (int r = 0; r < NA; ++r) {
+		C2 s = cmul(mt[NA * r], a[0]);
+#pragma unroll
+		for (int c = 1; c < NA; ++c)
+			s = cmad(mt[NA * r + c], a[c], s);
+		y[r] = s;
+	}
+#pragma unroll
+	for (int r = 0; r < NA; ++r)
+		a[r] = y[r];
+}
+
 /* One gate of a pass: a single jump on the host-computed entry code. */
 template <typename C2>
 __device__ __forceinline__ void apply_gate(C2 (&a)[NA], const PassCtx &pc, uint32_t code,
@@ -285,6 +308,8 @@ __device__ __forceinline__ void apply_gate(C2 (&a)[NA], const PassCtx &pc, uint3
 	case DK_GC_NEG1 + 3: g_neg1<0, true>(a, pc, lc, la); break;
 	case DK_GC_NEG1 + 4: g_neg1<1, true>(a, pc, lc, la); break;
 	case DK_GC_NEG1 + 5: g_neg1<2, true>(a, pc, lc, la); break;
+	case DK_GC_DENSE3 + 0: g_dense3<false>(a, pc, lc, la, mt); break;
+	case DK_GC_DENSE3 + 1: g_dense3<true>(a, pc, lc, la, mt); break;
 	default:
 		g_diagk(a, pc, lc, la, (info >> 6) & 3, info & 3, (info >> 2) & 3,
 			(info >> 4) & 3, mt);

@@ -83,6 +83,10 @@ struct dk_state {
 #define DK_TILE_BITS_C128 11
 #define DK_TILE_BITS_C64 11
 #define DK_PASS_BITS 3
+/* nibbles of a tile number (tile bits m >= 0, register <= 40 qubits) */
+#define DK_DEP_NIBBLES 10
+/* default pass-folding cost of one gate (FP64 FMAs per thread) */
+#define DK_FOLD_DEFAULT 96
 
 enum {
 	DK_GK_DENSE1 = 1,
@@ -124,7 +128,14 @@ enum {
 	DK_GC_DENSE2 = 30, /* + pair index: (0,1) (0,2) (1,0) (1,2) (2,0) (2,1) */
 	DK_GC_DIAGK = 36,
 	DK_GC_NEG1 = 37,
+	DK_GC_DENSE3 = 43, /* + 1 with controls inside the tile: 8x8 matrix in
+			    * register order (a fused run or a 3-qubit gate) */
+	DK_GC_DENSE3V = 45, /* tensor sweeps: 2^la matrices; lc packs la indices
+			     * (10 bits each) of tile conditions; the tile uses
+			     * matrix sum_j [condition j holds] 2^j */
 };
+/* most tile conditions of one variant entry */
+#define DK_VAR_MAX 3
 
 /* A pass: the gates [g0, g1) applied to the 8 amplitudes each thread
  * gathers from the shared tile.  The tile is stored under an XOR swizzle that
@@ -134,19 +145,25 @@ enum {
  * pm and OR.  The host precomputes these tables per pass. */
 typedef struct dk_pass_desc {
 	uint16_t g0, g1; /* gate range [g0, g1) */
-	uint32_t flags; /* bit 0: a gate of the pass has controls inside the tile */
+	uint32_t flags; /* DK_PASS_CTL | DK_PASS_WARP */
 	uint32_t sp[DK_PASS_BITS]; /* swizzled slot offset of pass bit j */
 	uint32_t pm[DK_PASS_BITS]; /* raw tile-index mask of pass bit j */
 	uint32_t slo[32], shi[16]; /* swizzled offsets of thread bits 0-4 / 5-8 */
 	uint32_t rlo[32], rhi[16]; /* raw tile-index bits of the same */
 } dk_pass_desc; /* 416 bytes */
 
+enum {
+	DK_PASS_CTL = 1u, /* a gate of the pass has controls inside the tile */
+	DK_PASS_WARP = 2u, /* the next pass maps the same tile bits to the warp
+			    * index: a warp barrier separates the two */
+};
+
 typedef struct dk_sweep_hdr {
 	int32_t m; /* tile bits */
 	int32_t n; /* register qubits */
 	int32_t npass, ngate;
 	int32_t all_touched; /* every tile has an unconditionally active gate */
-	int32_t pad;
+	int32_t mode; /* DK_SWEEP_SCALAR or DK_SWEEP_TENSOR */
 	uint64_t ntiles;
 	uint8_t qpos[16]; /* global bit of local bit j (ascending) */
 	uint32_t pass_off, gate_off, mat_off; /* byte offsets from the header */
@@ -154,6 +171,12 @@ typedef struct dk_sweep_hdr {
 	uint32_t cond_off, ncond; /* global-condition table */
 	uint32_t pad2[2];
 } dk_sweep_hdr;
+
+/* Sweep execution modes.  SCALAR: the gate list holds any kinds, applied
+ * by per-thread FP arithmetic on 8 register amplitudes.  TENSOR: every entry
+ * is an 8x8 matrix in register order (controls on non-pass tile bits and
+ * outside the tile in the descriptor), applied with FP64 tensor-core MMAs. */
+enum { DK_SWEEP_SCALAR = 0, DK_SWEEP_TENSOR = 1 };
 
 /* One step of a flush plan. */
 typedef struct dk_step {
@@ -185,6 +208,14 @@ typedef struct dk_plan_limits {
 	int max_passes;
 	int max_mat; /* complex entries */
 	int fuse; /* 0: one gate per sweep */
+	/* Pass folding: the cost of applying one gate on its own, in FP64 FMAs
+	 * per thread (8 amplitudes), against which runs of gates inside a pass
+	 * are replaced by their 8x8 product.  In: 0 = default, < 0 = off.
+	 * Out: the cost used, 0 = off. */
+	int fold;
+	/* Tensor sweeps (tiles of at least 8 qubits): in 0 = on, < 0 = off;
+	 * out 1 / 0. */
+	int tensor;
 } dk_plan_limits;
 
 void dk_plan_default_limits(int prec, unsigned n, dk_plan_limits *lim);

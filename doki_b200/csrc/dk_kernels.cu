@@ -56,6 +56,9 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 	__shared__ uint8_t sq[16];
 	__shared__ uint64_t soff[NA]; /* global offset of register bits (load / store) */
 	__shared__ uint32_t sro[NA]; /* swizzled slot offset of the same */
+	/* tile base index = OR over nibbles k of sdep[k][nibble k of the tile
+	 * number]: the tile number's bits deposited into the non-tile qubits */
+	__shared__ uint64_t sdep[DK_DEP_NIBBLES][16];
 
 	{ /* stage gates and matrices (in amplitude precision) */
 		const uint4 *src = reinterpret_cast<const uint4 *>(prog + h->gate_off);
@@ -81,6 +84,14 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		soff[r] = o;
 		sro[r] = swz<SW>((uint32_t)r << lanes);
 	}
+	for (int e = tid; e < DK_DEP_NIBBLES * 16; e += blockDim.x) {
+		uint64_t v = (uint64_t)(e & 15) << (4 * (e >> 4));
+		for (int j = 0; j < m; ++j) {
+			const int q = sq[j];
+			v = ((v >> q) << (q + 1)) | (v & ((1ull << q) - 1ull));
+		}
+		sdep[e >> 4][e & 15] = v;
+	}
 	uint64_t off_t = 0;
 	for (int j = 0; j < lanes; ++j)
 		if ((tid >> j) & 1u)
@@ -88,14 +99,15 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 	const uint32_t stid = swz<SW>(tid);
 	__syncthreads();
 	const uint64_t ntiles = h->ntiles;
+	const int ndep = (h->n - m + 3) >> 2;
 	const bool skip_idle = (in == out) && !h->all_touched;
 
 	auto tile_base = [&](uint64_t t) -> uint64_t {
-		uint64_t base = t;
-		for (int j = 0; j < m; ++j) {
-			const int q = sq[j];
-			base = ((base >> q) << (q + 1)) | (base & ((1ull << q) - 1ull));
-		}
+		uint64_t base = 0;
+#pragma unroll
+		for (int k = 0; k < DK_DEP_NIBBLES; ++k)
+			if (k < ndep)
+				base |= sdep[k][(t >> (4 * k)) & 15u];
 		return base;
 	};
 	/* next tile (>= t, stepping by the grid) with at least one active gate */
@@ -127,6 +139,16 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		}
 		cp_async_commit();
 	};
+	/* slot offsets of the next pass, loaded while the current one computes */
+	uint32_t nsgb, ns0, ns1, ns2;
+	auto pass_slots = [&](int p) {
+		const dk_pass_desc *pd = passes + p;
+		nsgb = __ldg(&pd->slo[tid & 31]) ^ __ldg(&pd->shi[tid >> 5]);
+		ns0 = __ldg(&pd->sp[0]);
+		ns1 = __ldg(&pd->sp[1]);
+		ns2 = __ldg(&pd->sp[2]);
+	};
+	pass_slots(0);
 
 	double insq = 0.0, outsq = 0.0;
 	uint64_t t = next_tile(blockIdx.x);
@@ -152,24 +174,20 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		C2 a[NA];
 		for (int p = 0; p < npass; ++p) {
 			const dk_pass_desc *pd = passes + p;
-			const uint32_t sgb = __ldg(&pd->slo[tid & 31]) ^ __ldg(&pd->shi[tid >> 5]);
-			const uint32_t s0 = __ldg(&pd->sp[0]), s1 = __ldg(&pd->sp[1]),
-				       s2 = __ldg(&pd->sp[2]);
-			uint32_t slot[NA];
+			const uint32_t sgb = nsgb, s0 = ns0, s1 = ns1, s2 = ns2;
 #pragma unroll
 			for (int r = 0; r < NA; ++r)
-				slot[r] = sgb ^ ((r & 1) ? s0 : 0u) ^ ((r & 2) ? s1 : 0u) ^
-					  ((r & 4) ? s2 : 0u);
-#pragma unroll
-			for (int r = 0; r < NA; ++r)
-				a[r] = tile[slot[r]];
+				a[r] = tile[sgb ^ ((r & 1) ? s0 : 0u) ^ ((r & 2) ? s1 : 0u) ^
+					    ((r & 4) ? s2 : 0u)];
 			if (p == 0) {
 #pragma unroll
 				for (int r = 0; r < NA; ++r)
 					insq += sqabs(a[r]);
 			}
+			pass_slots(p + 1 < npass ? p + 1 : 0);
+			const uint32_t pflags = __ldg(&pd->flags);
 			PassCtx pc;
-			if (__ldg(&pd->flags) & 1u) {
+			if (pflags & DK_PASS_CTL) {
 				pc.gb = __ldg(&pd->rlo[tid & 31]) | __ldg(&pd->rhi[tid >> 5]);
 				pc.p0 = __ldg(&pd->pm[0]);
 				pc.p1 = __ldg(&pd->pm[1]);
@@ -190,8 +208,13 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 			}
 #pragma unroll
 			for (int r = 0; r < NA; ++r)
-				tile[slot[r]] = a[r];
-			__syncthreads();
+				tile[sgb ^ ((r & 1) ? s0 : 0u) ^ ((r & 2) ? s1 : 0u) ^
+				     ((r & 4) ? s2 : 0u)] = a[r];
+			/* the flag is uniform over the block */
+			if (pflags & DK_PASS_WARP)
+				__syncwarp();
+			else
+				__syncthreads();
 		}
 #pragma unroll
 		for (int r = 0; r < NA; ++r)
@@ -212,6 +235,257 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 			__syncthreads(); /* this buffer is refilled two tiles later */
 		t = tn;
 		cur ^= 1;
+	}
+	cp_async_wait_all();
+	block_sum2(insq, outsq);
+	if (tid == 0) {
+		partials[2 * blockIdx.x] = insq;
+		partials[2 * blockIdx.x + 1] = outsq;
+	}
+}
+
+/* ---- tensor-core sweep --------------------------------------------------- */
+
+#ifndef DK_TC_MINB11
+#define DK_TC_MINB11 3
+#endif
+#ifndef DK_TC_MINB12
+#define DK_TC_MINB12 1
+#endif
+
+
+/* FP64 tensor-core MMA, D (8x8) += A (8x4, row-major) * B (4x8, column-major).
+ * Lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4)], D[l/4][2(l%4)+1]. */
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
+{
+	asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+	    : "+d"(d0), "+d"(d1)
+	    : "d"(a), "d"(b));
+}
+
+/* Sweep whose gate list holds only 8x8 matrices in register order (folded
+ * runs of gates, and single gates whose remaining controls lie off the pass
+ * bits or outside the tile).  A pass works on columns: the 8 amplitudes that
+ * differ only in the pass bits, one column per thread index as in k_sweep.
+ * A warp owns 32 columns and treats them as 4 groups of 8; each group is one
+ * real product  [yr; yi] = [[Mr, -Mi], [Mi, Mr]] [xr; xi]  (16x16 by 16x8),
+ * i.e. 2 row blocks x 4 k-steps of m8n8k4 FP64 MMAs.  Lane l gathers
+ * amplitudes l%4 and 4 + l%4 of column l/4 (its B fragments), holds matrix
+ * entries (l/4, l%4) and (l/4, 4 + l%4) (its A fragments, read through L1),
+ * and writes amplitude l/4 of columns 2(l%4) and 2(l%4)+1.  Entries with
+ * controls off the pass bits write only the columns whose tile index
+ * satisfies them; the others keep their values in the shared tile. */
+template <typename R, int SW, int M, int MINB>
+__global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
+	k_sweep_tc(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
+		   const unsigned char *__restrict__ prog, double *partials)
+{
+	typedef typename CT<R>::T C2;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const dk_sweep_hdr *h = reinterpret_cast<const dk_sweep_hdr *>(prog);
+	const int m = h->m;
+	const int lanes = m - PB;
+	const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+	const int npass = h->npass, ngate = h->ngate;
+	const uint32_t tn_amp = 1u << m;
+	const int ncond = (int)h->ncond;
+	const size_t gate_bytes = (size_t)ngate * sizeof(dk_gate_desc);
+	C2 *tile = reinterpret_cast<C2 *>(sm);
+	uint4 *sg = reinterpret_cast<uint4 *>(sm + sizeof(C2) * tn_amp);
+	dk_gate_cond *scond =
+		reinterpret_cast<dk_gate_cond *>(reinterpret_cast<unsigned char *>(sg) + gate_bytes);
+	const dk_pass_desc *passes = reinterpret_cast<const dk_pass_desc *>(prog + h->pass_off);
+	const double2 *mats = reinterpret_cast<const double2 *>(prog + h->mat_off);
+	__shared__ uint8_t sq[16];
+	__shared__ uint64_t soff[NA];
+	__shared__ uint32_t sro[NA];
+	__shared__ uint64_t sdep[DK_DEP_NIBBLES][16];
+
+	{
+		const uint4 *src = reinterpret_cast<const uint4 *>(prog + h->gate_off);
+		for (int i = tid; i < ngate; i += blockDim.x)
+			sg[i] = __ldg(src + i);
+		const uint4 *csrc = reinterpret_cast<const uint4 *>(prog + h->cond_off);
+		uint4 *cdst = reinterpret_cast<uint4 *>(scond);
+		for (int i = tid; i < ncond; i += blockDim.x)
+			cdst[i] = __ldg(csrc + i);
+		for (int i = tid; i < 16; i += blockDim.x)
+			sq[i] = h->qpos[i];
+	}
+	__syncthreads();
+	for (int r = tid; r < NA; r += blockDim.x) {
+		uint64_t o = 0;
+		for (int j = 0; j < PB; ++j)
+			if ((r >> j) & 1)
+				o |= 1ull << sq[lanes + j];
+		soff[r] = o;
+		sro[r] = swz<SW>((uint32_t)r << lanes);
+	}
+	for (int e = tid; e < DK_DEP_NIBBLES * 16; e += blockDim.x) {
+		uint64_t v = (uint64_t)(e & 15) << (4 * (e >> 4));
+		for (int j = 0; j < m; ++j) {
+			const int q = sq[j];
+			v = ((v >> q) << (q + 1)) | (v & ((1ull << q) - 1ull));
+		}
+		sdep[e >> 4][e & 15] = v;
+	}
+	uint64_t off_t = 0;
+	for (int j = 0; j < lanes; ++j)
+		if ((tid >> j) & 1u)
+			off_t |= 1ull << sq[j];
+	const uint32_t stid = swz<SW>(tid);
+	__syncthreads();
+	const uint64_t ntiles = h->ntiles;
+	const int ndep = (h->n - m + 3) >> 2;
+	const bool skip_idle = (in == out) && !h->all_touched;
+
+	auto tile_base = [&](uint64_t t) -> uint64_t {
+		uint64_t base = 0;
+#pragma unroll
+		for (int k = 0; k < DK_DEP_NIBBLES; ++k)
+			if (k < ndep)
+				base |= sdep[k][(t >> (4 * k)) & 15u];
+		return base;
+	};
+	auto next_tile = [&](uint64_t t) -> uint64_t {
+		for (; t < ntiles; t += gridDim.x) {
+			if (!skip_idle)
+				return t;
+			const uint64_t base = tile_base(t);
+			for (int g = 0; g < ngate; ++g) {
+				const uint32_t gi = sg[g].y & 0xffffu;
+				if (gi == 0xffffu)
+					return t;
+				const dk_gate_cond c = scond[gi];
+				if (((base & c.gc) == c.gc) && !(base & c.ga))
+					return t;
+			}
+		}
+		return ntiles;
+	};
+	auto prefetch = [&](uint64_t base) {
+		const uint64_t bo = base | off_t;
+#pragma unroll
+		for (int r = 0; r < NA; ++r) {
+			C2 *dst = tile + (stid ^ sro[r]);
+			if (sizeof(C2) == 16)
+				cp_async16(dst, in + (bo | soff[r]));
+			else
+				cp_async8(dst, in + (bo | soff[r]));
+		}
+		cp_async_commit();
+	};
+
+	double insq = 0.0, outsq = 0.0;
+	uint64_t t = next_tile(blockIdx.x);
+	if (t < ntiles)
+		prefetch(tile_base(t));
+	const uint32_t gl = lane >> 2, gk = lane & 3u;
+	while (t < ntiles) {
+		const uint64_t base = tile_base(t);
+		cp_async_wait_all();
+		__syncthreads();
+		if (skip_idle) {
+			/* only touched tiles reach here: their old |amp|^2 leaves csq */
+#pragma unroll
+			for (int r = 0; r < NA; ++r)
+				insq += sqabs(tile[stid ^ sro[r]]);
+		}
+		for (int p = 0; p < npass; ++p) {
+			const dk_pass_desc *pd = passes + p;
+			const uint32_t shw = __ldg(&pd->shi[warp]);
+			const uint32_t s0 = __ldg(&pd->sp[0]), s1 = __ldg(&pd->sp[1]),
+				       s2 = __ldg(&pd->sp[2]);
+			const uint32_t gj0 = ((gk & 1u) ? s0 : 0u) ^ ((gk & 2u) ? s1 : 0u);
+			const uint32_t gj1 = gj0 ^ s2;
+			const uint32_t sr = ((gl & 1u) ? s0 : 0u) ^ ((gl & 2u) ? s1 : 0u) ^
+					    ((gl & 4u) ? s2 : 0u);
+			const uint32_t pflags = __ldg(&pd->flags);
+			const int g1 = __ldg(&pd->g1);
+			for (int g = __ldg(&pd->g0); g < g1; ++g) {
+				const uint4 d = sg[g];
+				const uint32_t gi = d.y & 0xffffu;
+				if (gi != 0xffffu) {
+					const dk_gate_cond c = scond[gi];
+					if (((base & c.gc) != c.gc) || (base & c.ga))
+						continue;
+				}
+				const uint32_t code = d.x & 0xffffu;
+				uint32_t mi = d.x >> 16; /* whole 8x8 matrices */
+				if (code == DK_GC_DENSE3V) {
+					/* the tile's conditions pick one of 2^d.w products */
+					for (uint32_t c = 0; c < d.w; ++c) {
+						const dk_gate_cond cc = scond[(d.z >> (10 * c)) & 1023u];
+						if (((base & cc.gc) == cc.gc) && !(base & cc.ga))
+							mi += 1u << c;
+					}
+				}
+				const double2 *mt = mats + 64 * (size_t)mi + 8 * gl + gk;
+				const double2 e0 = __ldg(mt), e1 = __ldg(mt + 4);
+				const bool ctl = code == DK_GC_DENSE3 + 1;
+				/* two column groups at a time: their slots are disjoint
+				 * from the other groups' */
+#pragma unroll
+				for (int q0 = 0; q0 < 4; q0 += 2) {
+					double y[2][4];
+#pragma unroll
+					for (int h2 = 0; h2 < 2; ++h2) {
+						const int q = q0 + h2;
+						const uint32_t bg = __ldg(&pd->slo[(q << 3) | gl]) ^ shw;
+						const double2 x0 = to_c128(tile[bg ^ gj0]);
+						const double2 x1 = to_c128(tile[bg ^ gj1]);
+						double r0 = 0.0, r1 = 0.0, i0 = 0.0, i1 = 0.0;
+						dmma(r0, r1, e0.x, x0.x);
+						dmma(i0, i1, e0.y, x0.x);
+						dmma(r0, r1, e1.x, x1.x);
+						dmma(i0, i1, e1.y, x1.x);
+						dmma(r0, r1, -e0.y, x0.y);
+						dmma(i0, i1, e0.x, x0.y);
+						dmma(r0, r1, -e1.y, x1.y);
+						dmma(i0, i1, e1.x, x1.y);
+						y[h2][0] = r0;
+						y[h2][1] = r1;
+						y[h2][2] = i0;
+						y[h2][3] = i1;
+					}
+					__syncwarp(); /* the groups' gathers precede their writes */
+#pragma unroll
+					for (int h2 = 0; h2 < 2; ++h2)
+#pragma unroll
+						for (int e = 0; e < 2; ++e) {
+							const uint32_t col =
+								((q0 + h2) << 3) | (2u * gk + e);
+							if (ctl) {
+								const uint32_t raw = __ldg(&pd->rlo[col]) |
+										     __ldg(&pd->rhi[warp]);
+								if (!ctl_ok(raw, d.z, d.w))
+									continue;
+							}
+							const uint32_t bs = __ldg(&pd->slo[col]) ^ shw;
+							tile[bs ^ sr] = from_c128<C2>(
+								make_double2(y[h2][e], y[h2][2 + e]));
+						}
+				}
+				__syncwarp();
+			}
+			if (!(pflags & DK_PASS_WARP))
+				__syncthreads();
+		}
+		C2 a[NA];
+#pragma unroll
+		for (int r = 0; r < NA; ++r)
+			a[r] = tile[stid ^ sro[r]];
+		__syncthreads(); /* the buffer is free: start the next tile's copy */
+		const uint64_t tn = next_tile(t + gridDim.x);
+		if (tn < ntiles)
+			prefetch(tile_base(tn));
+		const uint64_t bo = base | off_t;
+#pragma unroll
+		for (int r = 0; r < NA; ++r) {
+			outsq += sqabs(a[r]);
+			__stcs(out + (bo | soff[r]), a[r]);
+		}
+		t = tn;
 	}
 	cp_async_wait_all();
 	block_sum2(insq, outsq);
@@ -717,6 +991,45 @@ static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dpr
 	return cudaGetLastError();
 }
 
+template <typename R, int SW, int M, int MINB>
+static cudaError_t run_sweep_tc(const void *in, void *out, const unsigned char *dprog,
+				const dk_sweep_hdr *hp, int num_sms, const Scratch &s,
+				cudaStream_t st, int *blocks_out)
+{
+	typedef typename CT<R>::T C2;
+	const int m = hp->m;
+	const size_t smem = (sizeof(C2) << m) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
+			    (size_t)hp->ncond * sizeof(dk_gate_cond);
+	auto kern = k_sweep_tc<R, SW, M, MINB>;
+	/* raised once to the device maximum, never lowered (see run_sweep) */
+	static std::once_flag once;
+	static cudaError_t set_err = cudaSuccess;
+	std::call_once(once, [&] {
+		int dev = 0, maxopt = 0;
+		cudaGetDevice(&dev);
+		set_err = cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+						 dev);
+		cudaFuncAttributes fa;
+		if (set_err == cudaSuccess)
+			set_err = cudaFuncGetAttributes(&fa, kern);
+		if (set_err == cudaSuccess)
+			set_err = cudaFuncSetAttribute(kern,
+						       cudaFuncAttributeMaxDynamicSharedMemorySize,
+						       maxopt - (int)fa.sharedSizeBytes);
+	});
+	cudaError_t e = set_err;
+	if (e != cudaSuccess)
+		return e;
+	uint64_t blocks = hp->ntiles;
+	const uint64_t cap = (uint64_t)num_sms * MINB;
+	if (blocks > cap)
+		blocks = cap;
+	kern<<<(int)blocks, 1 << (m - DK_PASS_BITS), smem, st>>>((const C2 *)in, (C2 *)out,
+								   dprog, s.partials);
+	*blocks_out = (int)blocks;
+	return cudaGetLastError();
+}
+
 cudaError_t launch_sweep(int prec, const void *in, void *out,
 			 const unsigned char *dprog, const dk_sweep_hdr *hp,
 			 const dk_scal *sc_in, dk_scal *sc_out, const Scratch &s,
@@ -726,6 +1039,25 @@ cudaError_t launch_sweep(int prec, const void *in, void *out,
 	const int m = hp->m;
 	int blocks = 0;
 	cudaError_t e;
+	if (hp->mode == DK_SWEEP_TENSOR) {
+		/* FP64 tensor-core passes; tiles of 8 to 12 bits */
+		if (prec == DK_C128)
+			e = m >= 12 ? run_sweep_tc<double, 3, 12, DK_TC_MINB12>(in, out, dprog, hp,
+										num_sms, s, st, &blocks)
+				    : run_sweep_tc<double, 3, 11, DK_TC_MINB11>(in, out, dprog, hp,
+										num_sms, s, st, &blocks);
+		else
+			e = m >= 12 ? run_sweep_tc<float, 4, 12, DK_TC_MINB12>(in, out, dprog, hp,
+									       num_sms, s, st, &blocks)
+				    : run_sweep_tc<float, 4, 11, DK_TC_MINB11>(in, out, dprog, hp,
+									       num_sms, s, st, &blocks);
+		if (e != cudaSuccess)
+			return e;
+		const int all = hp->all_touched || (in != out);
+		k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc_in, sc_out, FIN_GATE, all);
+		g_launches += 2;
+		return cudaGetLastError();
+	}
 	/* 12-bit tiles: one 512-thread CTA per SM, double-buffered; up to 11 bits:
 	 * two 256-thread CTAs per SM, one buffer each */
 	if (prec == DK_C128)

@@ -41,6 +41,8 @@ void dk_plan_default_limits(int prec, unsigned n, dk_plan_limits *lim)
 	lim->max_passes = 512;
 	lim->max_mat = 4096; /* complex entries: <= 64 KiB of a sweep's shared memory */
 	lim->fuse = 1;
+	lim->fold = lim->fold > 0 ? lim->fold : (lim->fold < 0 ? 0 : DK_FOLD_DEFAULT);
+	lim->tensor = lim->tensor < 0 ? 0 : 1;
 }
 
 /* Kind of a gate as executed by the sweep kernel. */
@@ -173,10 +175,11 @@ static uint32_t swizzle(uint32_t i, int sw)
 	return i ^ (f & ((1u << sw) - 1u));
 }
 
-static void pass_tables(dk_pass_desc *pd, const uint8_t *pb, int m, int sw)
+/* Per-pass address tables for an explicit thread-bit -> tile-bit map:
+ * thread bit j (j < nl) carries tile bit lane[j]. */
+static void pass_tables_lanes(dk_pass_desc *pd, const uint8_t *pb, const uint8_t *lane,
+			      int nl, int sw)
 {
-	uint8_t lane[32];
-	const int nl = lane_map(m, pb, sw, lane);
 	for (int j = 0; j < DK_PASS_BITS; j++) {
 		pd->pm[j] = 1u << pb[j];
 		pd->sp[j] = swizzle(pd->pm[j], sw);
@@ -199,10 +202,278 @@ static void pass_tables(dk_pass_desc *pd, const uint8_t *pb, int m, int sw)
 	}
 }
 
+static void pass_tables(dk_pass_desc *pd, const uint8_t *pb, int m, int sw)
+{
+	uint8_t lane[32];
+	const int nl = lane_map(m, pb, sw, lane);
+	pass_tables_lanes(pd, pb, lane, nl, sw);
+}
+
+/* Lane bits of the passes of a phase whose warp bits are W: every residue
+ * mod `res` present among the lane bits of a pass makes its quarter-warp
+ * (half-warp) accesses conflict free. */
+static int phase_score(const uint32_t *pmask, int cnt, uint32_t W, int m, int res)
+{
+	int score = 0;
+	for (int i = 0; i < cnt; i++) {
+		const uint32_t L = ((1u << m) - 1u) & ~pmask[i] & ~W;
+		uint32_t seen = 0;
+		for (int b = 0; b < m; b++)
+			if (L & (1u << b))
+				seen |= 1u << (b % res);
+		score += popc(seen) == res;
+	}
+	return score;
+}
+
+/* A phase: consecutive passes [0, cnt) whose pass bits all avoid the same
+ * `wbits` tile bits W, which every pass maps to the thread bits above the 5
+ * lane bits.  A warp then touches the same tile slots in every pass of the
+ * phase, so consecutive passes only need a warp barrier.  `need[i]` are the
+ * target bits of pass i; they are filled up to DK_PASS_BITS from the phase's
+ * union first (keeping it small), W is picked from the rest. */
+static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, int wbits,
+			int res, uint8_t (*pbits)[DK_PASS_BITS])
+{
+	uint32_t F = 0, pmask[64];
+	for (int i = 0; i < cnt; i++)
+		F |= need[i];
+	for (int bit = m - 1; popc(F) < DK_PASS_BITS && bit >= 0; bit--)
+		F |= 1u << bit;
+	for (int i = 0; i < cnt; i++) {
+		uint32_t P = need[i];
+		for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
+			if (F & (1u << bit))
+				P |= 1u << bit;
+		pmask[i] = P;
+		int j = 0;
+		for (int bit = 0; bit < m; bit++)
+			if (P & (1u << bit))
+				pbits[i][j++] = (uint8_t)bit;
+	}
+	/* warp bits: the subset of the free bits that keeps the most passes
+	 * conflict free (first one found on ties) */
+	const uint32_t pool = ((1u << m) - 1u) & ~F;
+	uint32_t W = 0;
+	int best = -1;
+	for (uint32_t x = pool;; x = (x - 1) & pool) {
+		if (popc(x) == wbits) {
+			const int sc = phase_score(pmask, cnt, x, m, res);
+			if (sc > best) {
+				best = sc;
+				W = x;
+			}
+		}
+		if (x == 0)
+			break;
+	}
+	for (int i = 0; i < cnt; i++) {
+		uint8_t lane[32], free_bits[32];
+		int nf = 0, nl = 0, taken[32] = { 0 };
+		const uint32_t L = ((1u << m) - 1u) & ~pmask[i] & ~W;
+		for (int b = 0; b < m; b++)
+			if (L & (1u << b))
+				free_bits[nf++] = (uint8_t)b;
+		for (int r = 0; r < res; r++)
+			for (int k = 0; k < nf; k++)
+				if (!taken[k] && free_bits[k] % res == r) {
+					lane[nl++] = free_bits[k];
+					taken[k] = 1;
+					break;
+				}
+		for (int k = 0; k < nf; k++)
+			if (!taken[k])
+				lane[nl++] = free_bits[k];
+		for (int b = 0; b < m; b++)
+			if (W & (1u << b))
+				lane[nl++] = (uint8_t)b;
+		pass_tables_lanes(&pd[i], pbits[i], lane, nl, res);
+		if (i + 1 < cnt)
+			pd[i].flags |= DK_PASS_WARP;
+	}
+}
+
+/* ---- pass folding ------------------------------------------------------ */
+
+typedef struct fold_params {
+	int dispatch; /* cost of one gate on its own (0: no folding) */
+	int max_mat; /* complex matrix entries of a sweep */
+	int tensor; /* every gate list entry is an 8x8 product (tensor sweep) */
+} fold_params;
+
+/* An entry of a sweep's gate list: a source gate (op >= 0) or a folded run
+ * (op < 0); m8 is the 8x8 matrix in register order for DK_GK_DENSE3. */
+typedef struct item_t {
+	int op, kind, pass;
+	int m8; /* first 8x8 matrix (register order) in the matrix buffer, -1: none */
+	int nmat; /* matrices: 1, or 2^nvar for a variant entry */
+	int nvar; /* variant entry: tile conditions cgc/cga[0..nvar) select the matrix */
+	int has_cond; /* plain entry applied where cgc/cga[0] holds */
+	uint64_t cgc[DK_VAR_MAX], cga[DK_VAR_MAX];
+} item_t;
+
+/* growable buffer of 8x8 complex matrices (128 doubles each) */
+typedef struct mbuf_t {
+	double *p;
+	int n, cap;
+} mbuf_t;
+
+static int mbuf_add(mbuf_t *mb, int count)
+{
+	if (mb->n + count > mb->cap) {
+		int nc = mb->cap ? mb->cap : 64;
+		while (nc < mb->n + count)
+			nc *= 2;
+		double *np = (double *)realloc(mb->p, sizeof(double) * 128 * (size_t)nc);
+		if (!np)
+			return -1;
+		mb->p = np;
+		mb->cap = nc;
+	}
+	const int at = mb->n;
+	mb->n += count;
+	return at;
+}
+
+/* Tensor sweeps: a gate folds into a pass matrix when its targets and its
+ * in-tile controls are pass bits; controls outside the tile become tile
+ * conditions (matrix variants). */
+static int tc_local(const dk_flat_op *op, const int8_t *loc_of, const uint32_t *preg)
+{
+	for (unsigned t = 0; t < op->k; t++) {
+		const int lb = loc_of[op->tg[t]];
+		if (lb < 0 || preg[lb] == 0xffffffffu)
+			return 0;
+	}
+	const uint64_t c = op->cm | op->am;
+	for (unsigned q = 0; q < 64; q++)
+		if ((c >> q & 1u) && loc_of[q] >= 0 && preg[loc_of[q]] == 0xffffffffu)
+			return 0;
+	return 1;
+}
+
+static void tile_cond(const dk_flat_op *op, const int8_t *loc_of, unsigned n, uint64_t *gc,
+		      uint64_t *ga)
+{
+	*gc = *ga = 0;
+	for (unsigned q = 0; q < n; q++) {
+		if (loc_of[q] >= 0)
+			continue;
+		const uint64_t bit = UINT64_C(1) << q;
+		if (op->cm & bit)
+			*gc |= bit;
+		if (op->am & bit)
+			*ga |= bit;
+	}
+}
+
+/* FP64 FMAs per thread (8 amplitudes) of one gate of each kind */
+static int fold_cost(int kind)
+{
+	switch (kind) {
+	case DK_GK_DENSE1: return 64;
+	case DK_GK_DENSE2: return 128;
+	case DK_GK_DENSE3: return 256;
+	case DK_GK_DIAG1:
+	case DK_GK_ANTI1:
+	case DK_GK_DIAGK: return 32;
+	case DK_GK_PHASE1: return 16;
+	default: return 0; /* SWAP1, NEG1: moves and sign flips */
+	}
+}
+
+/* A gate folds into the 8x8 matrix of a pass when its targets and all its
+ * controls are bits of the pass (preg[tile bit] = register bit, or ~0). */
+static int foldable(const dk_flat_op *op, const int8_t *loc_of, const uint32_t *preg)
+{
+	for (unsigned t = 0; t < op->k; t++) {
+		const int lb = loc_of[op->tg[t]];
+		if (lb < 0 || preg[lb] == 0xffffffffu)
+			return 0;
+	}
+	const uint64_t c = op->cm | op->am;
+	for (unsigned q = 0; q < 64; q++)
+		if (c & (UINT64_C(1) << q)) {
+			const int lb = loc_of[q];
+			if (lb < 0 || preg[lb] == 0xffffffffu)
+				return 0;
+		}
+	return 1;
+}
+
+static void identity8(double *M)
+{
+	memset(M, 0, sizeof(double) * 128);
+	for (int r = 0; r < 8; r++)
+		M[2 * (8 * r + r)] = 1.0;
+}
+
+/* 8x8 matrix, in register order, of a gate on the pass's bits: entry (r, c)
+ * is the gate's entry (row(r), row(c)) where r and c agree outside the target
+ * bits and the controls on pass bits hold on c, the identity elsewhere.
+ * row(x) gathers the target bits of x, targets[0] lowest.  Controls off the
+ * pass bits are left to the gate descriptor. */
+static void gate8(const dk_flat_op *op, const int8_t *loc_of, const uint32_t *preg, double *G)
+{
+	unsigned treg[DK_SWEEP_MAX_K], tmask = 0, cr = 0, ar = 0;
+	for (unsigned t = 0; t < op->k; t++) {
+		treg[t] = preg[loc_of[op->tg[t]]];
+		tmask |= 1u << treg[t];
+	}
+	for (unsigned q = 0; q < 64; q++) {
+		const uint64_t bit = UINT64_C(1) << q;
+		if (!((op->cm | op->am) & bit) || loc_of[q] < 0 ||
+		    preg[loc_of[q]] == 0xffffffffu)
+			continue;
+		if (op->cm & bit)
+			cr |= 1u << preg[loc_of[q]];
+		else
+			ar |= 1u << preg[loc_of[q]];
+	}
+	const uint64_t d = op->gate->dim;
+	const double *g = op->gate->m;
+	memset(G, 0, sizeof(double) * 128);
+	for (unsigned r = 0; r < 8; r++)
+		for (unsigned c = 0; c < 8; c++) {
+			if ((r & ~tmask) != (c & ~tmask))
+				continue;
+			double *e = G + 2 * (8 * r + c);
+			if ((c & cr) != cr || (c & ar)) {
+				e[0] = (r == c) ? 1.0 : 0.0;
+				continue;
+			}
+			unsigned gr = 0, gcn = 0;
+			for (unsigned t = 0; t < op->k; t++) {
+				gr |= ((r >> treg[t]) & 1u) << t;
+				gcn |= ((c >> treg[t]) & 1u) << t;
+			}
+			e[0] = g[2 * (gr * d + gcn)];
+			e[1] = g[2 * (gr * d + gcn) + 1];
+		}
+}
+
+/* M = G * M (8x8 complex, row-major, interleaved) */
+static void mul8(const double *G, double *M)
+{
+	double T[128];
+	for (int r = 0; r < 8; r++)
+		for (int c = 0; c < 8; c++) {
+			double re = 0.0, im = 0.0;
+			for (int k = 0; k < 8; k++) {
+				const double *a = G + 2 * (8 * r + k), *b = M + 2 * (8 * k + c);
+				re += a[0] * b[0] - a[1] * b[1];
+				im += a[0] * b[1] + a[1] * b[0];
+			}
+			T[2 * (8 * r + c)] = re;
+			T[2 * (8 * r + c) + 1] = im;
+		}
+	memcpy(M, T, sizeof(T));
+}
+
 /* Emit one sweep program for ops[idx[0..cnt)] over tile set Q. */
 static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		      int cnt, uint64_t Q, unsigned n, int prec, int m,
-		      const int *kinds, dk_step *step)
+		      const int *kinds, const fold_params *fold, dk_step *step)
 {
 	uint8_t qpos[64];
 	int8_t loc_of[64];
@@ -224,12 +495,14 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		(dk_pass_desc *)calloc((size_t)(cnt ? cnt : 1), sizeof(dk_pass_desc));
 	uint8_t(*pbits)[DK_PASS_BITS] =
 		(uint8_t(*)[DK_PASS_BITS])calloc((size_t)(cnt ? cnt : 1), DK_PASS_BITS);
-	if (!rem || !defer || !order || !passes || !pbits) {
+	uint32_t *need = (uint32_t *)calloc((size_t)(cnt ? cnt : 1), sizeof(uint32_t));
+	if (!rem || !defer || !order || !passes || !pbits || !need) {
 		free(rem);
 		free(defer);
 		free(order);
 		free(passes);
 		free(pbits);
+		free(need);
 		return -1;
 	}
 	int nrem = cnt, npass = 0, nord = 0;
@@ -254,6 +527,17 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 			uint32_t tl = 0;
 			for (unsigned t = 0; t < op->k; t++)
 				tl |= 1u << loc_of[op->tg[t]];
+			if (fold->tensor) {
+				/* tensor sweeps: keep a gate's in-tile controls in its
+				 * pass when they fit, so the gate folds into the pass
+				 * matrix instead of needing a product of its own */
+				uint32_t sl = tl;
+				for (unsigned q = 0; q < n; q++)
+					if (((op->cm | op->am) >> q & 1u) && loc_of[q] >= 0)
+						sl |= 1u << loc_of[q];
+				if (popc(sl) <= DK_PASS_BITS)
+					tl = sl;
+			}
 			if (popc(P | tl) <= DK_PASS_BITS) {
 				P |= tl;
 				order[nord++] = rem[i];
@@ -263,47 +547,215 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 			}
 		}
 		pd->g1 = (uint16_t)nord;
-		/* fill the pass up to DK_PASS_BITS bits with the highest free tile bits */
-		for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
-			P |= 1u << bit;
-		int j = 0;
-		for (int bit = 0; bit < m; bit++)
-			if (P & (1u << bit))
-				pbits[npass][j++] = (uint8_t)bit;
-		pass_tables(pd, pbits[npass], m, res);
+		need[npass] = P;
 		for (int g = pd->g0; g < pd->g1; g++) {
 			const dk_flat_op *op = &ops[order[g]];
 			if ((op->cm | op->am) & Q)
-				pd->flags |= 1u;
+				pd->flags |= DK_PASS_CTL;
 		}
 		npass++;
 		memcpy(rem, defer, sizeof(int) * (size_t)nd);
 		nrem = nd;
 	}
 
-	/* size the program */
-	int nmat = 0;
-	for (int i = 0; i < nord; i++)
-		nmat += mat_entries(kinds[order[i]], ops[order[i]].k);
-	int ncond = 0;
-	for (int i = 0; i < nord; i++) {
-		const dk_flat_op *op = &ops[order[i]];
-		if ((op->cm | op->am) & ~Q)
-			ncond++;
+	/* Pass bits and lane tables.  With at least one full warp per tile
+	 * (m >= 8) passes are grouped into warp phases: a run of passes whose
+	 * target bits fit in m - wbits tile bits (wbits = thread bits above the
+	 * lanes).  Narrower tiles fill each pass with the highest free bits. */
+	const int wbits = m - DK_PASS_BITS - 5;
+	for (int p0 = 0; p0 < npass;) {
+		int p1 = p0 + 1;
+		if (wbits >= 0) {
+			uint32_t U = need[p0];
+			while (p1 < npass && p1 - p0 < 64 && popc(U | need[p1]) <= m - wbits)
+				U |= need[p1++];
+			build_phase(&passes[p0], &need[p0], p1 - p0, m, wbits, res, &pbits[p0]);
+		} else {
+			uint32_t P = need[p0];
+			for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
+				P |= 1u << bit;
+			int j = 0;
+			for (int bit = 0; bit < m; bit++)
+				if (P & (1u << bit))
+					pbits[p0][j++] = (uint8_t)bit;
+			pass_tables(&passes[p0], pbits[p0], m, res);
+		}
+		p0 = p1;
 	}
-	size_t pass_off = align_up(sizeof(dk_sweep_hdr), 16);
-	size_t gate_off = align_up(pass_off + sizeof(dk_pass_desc) * (size_t)npass, 16);
-	size_t cond_off = align_up(gate_off + sizeof(dk_gate_desc) * (size_t)nord, 16);
-	size_t mat_off = align_up(cond_off + sizeof(dk_gate_cond) * (size_t)ncond, 16);
-	size_t bytes = align_up(mat_off + 16 * (size_t)nmat, 16);
 
-	size_t start = align_up(b->len, 16);
-	if (blob_reserve(b, (start - b->len) + bytes)) {
+	/* Gate-list entries.  Scalar sweeps: a run of consecutive gates of a
+	 * pass that act only on the pass's bits (targets and controls) and on
+	 * every tile is replaced by its 8x8 product when that is cheaper than
+	 * applying the gates one by one; dense 3-qubit gates are stored in
+	 * register order.  Tensor sweeps: every entry is 8x8; a run of gates
+	 * whose targets and in-tile controls are pass bits becomes one entry,
+	 * with one matrix per combination of the run's (at most DK_VAR_MAX)
+	 * distinct conditions on qubits outside the tile. */
+	item_t *items = (item_t *)calloc((size_t)(nord ? nord : 1), sizeof(item_t));
+	mbuf_t mb = { NULL, 0, 0 };
+	if (!items) {
 		free(rem);
 		free(defer);
 		free(order);
 		free(passes);
 		free(pbits);
+		free(need);
+		return -1;
+	}
+	int nit = 0, tot_mat = 0, oom = 0;
+	for (int i = 0; i < nord; i++)
+		tot_mat += mat_entries(kinds[order[i]], ops[order[i]].k);
+	for (int pi = 0; pi < npass && !oom; pi++) {
+		const int g0 = passes[pi].g0, g1 = passes[pi].g1;
+		uint32_t preg[64];
+		memset(preg, 0xff, sizeof(preg));
+		for (int r = 0; r < DK_PASS_BITS; r++)
+			preg[pbits[pi][r]] = (uint32_t)r;
+		passes[pi].g0 = (uint16_t)nit;
+		for (int g = g0; g < g1 && !oom;) {
+			item_t *it = &items[nit];
+			memset(it, 0, sizeof(*it));
+			it->pass = pi;
+			it->m8 = -1;
+			if (fold->tensor && tc_local(&ops[order[g]], loc_of, preg)) {
+				int e = g, all_cond = 1;
+				while (e < g1 && tc_local(&ops[order[e]], loc_of, preg)) {
+					uint64_t gc, ga;
+					tile_cond(&ops[order[e]], loc_of, n, &gc, &ga);
+					if (gc | ga) {
+						int j = 0;
+						while (j < it->nvar && (it->cgc[j] != gc || it->cga[j] != ga))
+							j++;
+						if (j == it->nvar) {
+							if (it->nvar == DK_VAR_MAX)
+								break;
+							it->cgc[j] = gc;
+							it->cga[j] = ga;
+							it->nvar++;
+						}
+					} else {
+						all_cond = 0;
+					}
+					e++;
+				}
+				/* one condition shared by every gate of the run: a plain
+				 * entry skipped by the other tiles */
+				if (it->nvar == 1 && all_cond) {
+					it->nvar = 0;
+					it->has_cond = 1;
+				}
+				it->op = -1;
+				it->kind = DK_GK_DENSE3;
+				it->nmat = 1 << it->nvar;
+				it->m8 = mbuf_add(&mb, it->nmat);
+				if (it->m8 < 0) {
+					oom = 1;
+					break;
+				}
+				for (int v = 0; v < it->nmat; v++) {
+					double *M = mb.p + 128 * (size_t)(it->m8 + v);
+					identity8(M);
+					for (int j = g; j < e; j++) {
+						uint64_t gc, ga;
+						tile_cond(&ops[order[j]], loc_of, n, &gc, &ga);
+						int on = 1;
+						for (int c = 0; c < it->nvar; c++)
+							if (it->cgc[c] == gc && it->cga[c] == ga)
+								on = (v >> c) & 1;
+						if (!on)
+							continue;
+						double G[128];
+						gate8(&ops[order[j]], loc_of, preg, G);
+						mul8(G, M);
+					}
+				}
+				nit++;
+				g = e;
+				continue;
+			}
+			if (!fold->tensor) {
+				int e = g, run_cost = 0, run_mat = 0;
+				while (e < g1 && foldable(&ops[order[e]], loc_of, preg)) {
+					run_cost += fold_cost(kinds[order[e]]) + fold->dispatch;
+					run_mat += mat_entries(kinds[order[e]], ops[order[e]].k);
+					e++;
+				}
+				const int fused_cost = fold_cost(DK_GK_DENSE3) + fold->dispatch;
+				if (e - g >= 2 && fold->dispatch > 0 && run_cost > fused_cost &&
+				    tot_mat - run_mat + 64 <= fold->max_mat) {
+					it->op = -1;
+					it->kind = DK_GK_DENSE3;
+					it->nmat = 1;
+					it->m8 = mbuf_add(&mb, 1);
+					if (it->m8 < 0) {
+						oom = 1;
+						break;
+					}
+					double *M = mb.p + 128 * (size_t)it->m8;
+					identity8(M);
+					for (int j = g; j < e; j++) {
+						double G[128];
+						gate8(&ops[order[j]], loc_of, preg, G);
+						mul8(G, M);
+					}
+					tot_mat += 64 - run_mat;
+					nit++;
+					g = e;
+					continue;
+				}
+			}
+			/* a single gate; 8x8 in register order when it is a dense
+			 * 3-qubit gate or the sweep is a tensor sweep */
+			it->op = order[g];
+			it->kind = kinds[order[g]];
+			if (it->kind == DK_GK_DENSE3 || fold->tensor) {
+				it->kind = DK_GK_DENSE3;
+				it->nmat = 1;
+				it->m8 = mbuf_add(&mb, 1);
+				if (it->m8 < 0) {
+					oom = 1;
+					break;
+				}
+				gate8(&ops[order[g]], loc_of, preg, mb.p + 128 * (size_t)it->m8);
+			}
+			nit++;
+			g++;
+		}
+		passes[pi].g1 = (uint16_t)nit;
+		/* controls inside the tile, after folding */
+		passes[pi].flags &= ~(uint32_t)DK_PASS_CTL;
+		for (int k = passes[pi].g0; k < nit; k++) {
+			const dk_flat_op *op = items[k].op >= 0 ? &ops[items[k].op] : NULL;
+			if (op && ((op->cm | op->am) & Q))
+				passes[pi].flags |= DK_PASS_CTL;
+		}
+	}
+
+	/* size the program */
+	int nmat = 0, ncond = 0;
+	for (int i = 0; i < nit; i++) {
+		nmat += items[i].m8 >= 0 ? 64 * items[i].nmat
+					 : mat_entries(items[i].kind, ops[items[i].op].k);
+		ncond += items[i].nvar + items[i].has_cond;
+		if (items[i].op >= 0 && ((ops[items[i].op].cm | ops[items[i].op].am) & ~Q))
+			ncond++;
+	}
+	size_t pass_off = align_up(sizeof(dk_sweep_hdr), 16);
+	size_t gate_off = align_up(pass_off + sizeof(dk_pass_desc) * (size_t)npass, 16);
+	size_t cond_off = align_up(gate_off + sizeof(dk_gate_desc) * (size_t)nit, 16);
+	size_t mat_off = align_up(cond_off + sizeof(dk_gate_cond) * (size_t)ncond, 16);
+	size_t bytes = align_up(mat_off + 16 * (size_t)nmat, 16);
+
+	size_t start = align_up(b->len, 16);
+	if (oom || blob_reserve(b, (start - b->len) + bytes)) {
+		free(items);
+		free(mb.p);
+		free(rem);
+		free(defer);
+		free(order);
+		free(passes);
+		free(pbits);
+		free(need);
 		return -1;
 	}
 	memset(b->p + b->len, 0, (start - b->len) + bytes);
@@ -313,7 +765,7 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	h->m = m;
 	h->n = (int32_t)n;
 	h->npass = npass;
-	h->ngate = nord;
+	h->ngate = nit;
 	h->ntiles = UINT64_C(1) << (n - (unsigned)m);
 	memcpy(h->qpos, qpos, (size_t)m);
 	h->pass_off = (uint32_t)pass_off;
@@ -328,13 +780,72 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	dk_gate_cond *conds = (dk_gate_cond *)(base + cond_off);
 	double *mats = (double *)(base + mat_off);
 	int moff = 0, all_touched = 0, ci = 0;
-	int pi = 0;
-	for (int i = 0; i < nord; i++) {
-		while (pi < npass && i >= passes[pi].g1)
-			pi++;
-		const dk_flat_op *op = &ops[order[i]];
-		const int kind = kinds[order[i]];
+	for (int i = 0; i < nit; i++) {
+		const int pi = items[i].pass;
+		const int kind = items[i].kind;
 		dk_gate_desc *g = &gd[i];
+		/* tensor sweeps count matrix offsets in whole 8x8 matrices */
+		g->mat = (uint16_t)(fold->tensor ? moff / 64 : moff);
+		if (items[i].m8 >= 0) {
+			/* 8x8 matrices in register order: fused runs, variants or a
+			 * single gate whose controls on the pass bits are inside */
+			uint64_t gc = 0, ga = 0;
+			if (items[i].op >= 0) {
+				const dk_flat_op *op = &ops[items[i].op];
+				uint32_t pmask = 0;
+				for (int r = 0; r < DK_PASS_BITS; r++)
+					pmask |= 1u << pbits[pi][r];
+				for (unsigned q = 0; q < n; q++) {
+					uint64_t bit = UINT64_C(1) << q;
+					if (loc_of[q] >= 0 && (pmask >> loc_of[q] & 1u))
+						continue;
+					if (op->cm & bit) {
+						if (loc_of[q] >= 0)
+							g->lc |= 1u << loc_of[q];
+						else
+							gc |= bit;
+					}
+					if (op->am & bit) {
+						if (loc_of[q] >= 0)
+							g->la |= 1u << loc_of[q];
+						else
+							ga |= bit;
+					}
+				}
+			} else if (items[i].has_cond) {
+				gc = items[i].cgc[0];
+				ga = items[i].cga[0];
+			}
+			if (gc == 0 && ga == 0) {
+				all_touched = 1;
+				g->gcond = 0xffff;
+			} else {
+				conds[ci].gc = gc;
+				conds[ci].ga = ga;
+				g->gcond = (uint16_t)ci++;
+			}
+			if (items[i].nvar > 0) {
+				/* variant entry: lc packs the condition indices (10 bits
+				 * each), la their count */
+				g->lc = 0;
+				for (int c = 0; c < items[i].nvar; c++) {
+					conds[ci].gc = items[i].cgc[c];
+					conds[ci].ga = items[i].cga[c];
+					g->lc |= (uint32_t)ci++ << (10 * c);
+				}
+				g->la = (uint32_t)items[i].nvar;
+				g->code = (uint16_t)DK_GC_DENSE3V;
+			} else {
+				g->code = (uint16_t)(DK_GC_DENSE3 + ((g->lc | g->la) != 0));
+			}
+			g->info = (uint16_t)(0 | (1 << 2) | (2 << 4) | (3u << 6) |
+					     ((unsigned)DK_GK_DENSE3 << 8));
+			memcpy(mats + 2 * moff, mb.p + 128 * (size_t)items[i].m8,
+			       sizeof(double) * 128 * (size_t)items[i].nmat);
+			moff += 64 * items[i].nmat;
+			continue;
+		}
+		const dk_flat_op *op = &ops[items[i].op];
 		uint8_t treg[3] = { 0, 0, 0 };
 		for (unsigned t = 0; t < op->k; t++) {
 			int lb = loc_of[op->tg[t]];
@@ -383,7 +894,6 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		}
 		g->info = (uint16_t)(treg[0] | (treg[1] << 2) | (treg[2] << 4) |
 				     ((op->k & 3u) << 6) | ((unsigned)kind << 8));
-		g->mat = (uint16_t)moff;
 		const double *src = op->gate->m;
 		const uint64_t d = op->gate->dim;
 		double *dst = mats + 2 * moff;
@@ -412,16 +922,20 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		moff += mat_entries(kind, op->k);
 	}
 	h->all_touched = all_touched;
+	h->mode = fold->tensor ? DK_SWEEP_TENSOR : DK_SWEEP_SCALAR;
 	b->len = start + bytes;
 	step->kind = 1;
 	step->prog_off = start;
 	step->op_index = -1;
 	step->ngates = nord;
+	free(items);
+	free(mb.p);
 	free(rem);
 	free(defer);
 	free(order);
 	free(passes);
 	free(pbits);
+	free(need);
 	return 0;
 }
 
@@ -441,15 +955,14 @@ int dk_plan_build(const dk_flat_op *ops, int nops, unsigned n, int prec,
 		goto fail;
 	const int m = lim->tile_bits;
 	const int sweepable = (m >= DK_PASS_BITS);
+	/* tensor sweeps need a full warp of 8-amplitude columns per tile */
+	const fold_params fold = { lim->fold > 0 ? lim->fold : 0, lim->max_mat,
+				   lim->tensor > 0 && m >= DK_PASS_BITS + 5 };
 	for (int i = 0; i < nops; i++) {
 		rem[i] = i;
 		kinds[i] = (ops[i].k <= DK_SWEEP_MAX_K && sweepable)
 				   ? dk_gate_classify(ops[i].gate)
 				   : 0;
-		/* dense 3-qubit gates run as generic steps (kept out of the
-		 * register budget of the sweep) */
-		if (kinds[i] == DK_GK_DENSE3)
-			kinds[i] = 0;
 	}
 	int nrem = nops, nsteps = 0;
 	while (nrem > 0) {
@@ -504,7 +1017,7 @@ int dk_plan_build(const dk_flat_op *ops, int nops, unsigned n, int prec,
 		/* complete Q to m bits with the lowest free qubits */
 		for (unsigned q = 0; popc(Q) < m && q < n; q++)
 			Q |= UINT64_C(1) << q;
-		if (emit_sweep(&b, ops, take, nt, Q, n, prec, m, kinds,
+		if (emit_sweep(&b, ops, take, nt, Q, n, prec, m, kinds, &fold,
 			       &steps[nsteps]))
 			goto fail;
 		nsteps++;

@@ -53,6 +53,8 @@ struct Ctx {
 	size_t budget = 0; /* 0 = unlimited */
 	int fuse = 1;
 	int tile_bits = 0; /* 0: planner default */
+	int fold = 0; /* pass-folding cost: 0 planner default, < 0 off */
+	int tensor = 0; /* tensor-core sweeps: 0 planner default (on), < 0 off */
 	std::atomic<unsigned long long> sweeps{ 0 }, gates{ 0 }, h2d{ 0 }, d2h{ 0 };
 	char err[256] = { 0 };
 };
@@ -265,6 +267,8 @@ int flush(dk_state *s)
 	}
 	dk_plan_limits lim = {};
 	lim.tile_bits = g.tile_bits;
+	lim.fold = g.fold;
+	lim.tensor = g.tensor;
 	dk_plan_default_limits(prec, n, &lim);
 	lim.fuse = g.fuse;
 	dk_plan plan;
@@ -511,6 +515,12 @@ int dk_init(int device)
 	const char *f = getenv("DK_FUSE");
 	if (f)
 		g.fuse = atoi(f) ? 1 : 0;
+	const char *fo = getenv("DK_FOLD");
+	if (fo)
+		g.fold = atoi(fo);
+	const char *te = getenv("DK_TENSOR");
+	if (te)
+		g.tensor = atoi(te) ? 0 : -1;
 	g.inited = 1;
 	return DK_OK;
 }

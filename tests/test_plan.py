@@ -29,7 +29,8 @@ class FlatOp(ctypes.Structure):
 class Limits(ctypes.Structure):
     _fields_ = [("tile_bits", ctypes.c_int), ("low_bits", ctypes.c_int),
                 ("max_gates", ctypes.c_int), ("max_passes", ctypes.c_int),
-                ("max_mat", ctypes.c_int), ("fuse", ctypes.c_int)]
+                ("max_mat", ctypes.c_int), ("fuse", ctypes.c_int),
+                ("fold", ctypes.c_int), ("tensor", ctypes.c_int)]
 
 
 class Step(ctypes.Structure):
@@ -43,7 +44,7 @@ class Plan(ctypes.Structure):
 
 
 HDR = np.dtype([("m", "<i4"), ("n", "<i4"), ("npass", "<i4"), ("ngate", "<i4"),
-                ("all_touched", "<i4"), ("pad", "<i4"), ("ntiles", "<u8"),
+                ("all_touched", "<i4"), ("mode", "<i4"), ("ntiles", "<u8"),
                 ("qpos", "u1", 16), ("pass_off", "<u4"), ("gate_off", "<u4"),
                 ("mat_off", "<u4"), ("bytes", "<u4"), ("cond_off", "<u4"),
                 ("ncond", "<u4"), ("pad2", "<u4", 2)])
@@ -68,7 +69,7 @@ def lib():
     return L
 
 
-def build_plan(lib, ops, n, prec=2, fuse=1, tile_bits=None):
+def build_plan(lib, ops, n, prec=2, fuse=1, tile_bits=None, fold=0, tensor=0):
     gates, flat = [], (FlatOp * len(ops))()
     for i, op in enumerate(ops):
         m = np.ascontiguousarray(op.gate, dtype=np.complex128)
@@ -82,6 +83,8 @@ def build_plan(lib, ops, n, prec=2, fuse=1, tile_bits=None):
         flat[i].cm = sum(1 << c for c in op.controls)
         flat[i].am = sum(1 << c for c in op.anticontrols)
     lim = Limits()
+    lim.fold = fold
+    lim.tensor = tensor
     lib.dk_plan_default_limits(prec, n, ctypes.byref(lim))
     lim.fuse = fuse
     if tile_bits is not None:
@@ -122,6 +125,9 @@ def assert_code(code, kind, treg, ctl):
     elif kind == 4:
         pairs = [(0, 1), (0, 2), (1, 0), (1, 2), (2, 0), (2, 1)]
         assert code == 30 + pairs.index((treg[0], treg[1]))
+    elif kind == 5:
+        assert code in (43, 44, 45) and treg == [0, 1, 2]
+        assert code == 45 or code == 43 + (ctl != 0)
     else:
         assert kind == 6 and code == 36
 
@@ -135,6 +141,7 @@ def replay_sweep(blob, off, psi):
     conds = np.frombuffer(blob, COND, int(h["ncond"]), off + int(h["cond_off"]))
     nmat = (int(h["bytes"]) - int(h["mat_off"])) // 16
     mats = np.frombuffer(blob, np.complex128, nmat, off + int(h["mat_off"]))
+    tensor = int(h["mode"]) == 1
     qmask = sum(1 << q for q in qpos)
     out = psi.copy()
     local = np.arange(1 << m)
@@ -154,13 +161,22 @@ def replay_sweep(blob, off, psi):
                     if (base & gc) != gc or (base & ga):
                         continue
                 lc, la = int(g["lc"]), int(g["la"])
-                ok = ((local & lc) == lc) & ((local & la) == 0)
                 info = int(g["info"])
                 k = (info >> 6) & 3
                 treg = [info & 3, (info >> 2) & 3, (info >> 4) & 3]
                 tb = [int(p["pm"][treg[j]]).bit_length() - 1 for j in range(k)]
-                kind, mo = info >> 8, int(g["mat"])
+                kind, mo = info >> 8, int(g["mat"]) * (64 if tensor else 1)
                 assert_code(int(g["code"]), kind, treg, lc | la)
+                if int(g["code"]) == 45:
+                    # variant entry: the tile's conditions select the matrix
+                    assert tensor and 1 <= la <= 3
+                    for c in range(la):
+                        cc = conds[(lc >> (10 * c)) & 1023]
+                        gc, ga = int(cc["gc"]), int(cc["ga"])
+                        if (base & gc) == gc and not (base & ga):
+                            mo += 64 << c
+                    lc = la = 0
+                ok = ((local & lc) == lc) & ((local & la) == 0)
                 if kind == 1 or kind == 4 or kind == 5:
                     mat = mats[mo:mo + (1 << 2 * k)].reshape(1 << k, 1 << k)
                 elif kind == 2:
@@ -228,15 +244,17 @@ def random_ops(rng, n, count, kmax=3):
     return ops
 
 
-@pytest.mark.parametrize("n,tile_bits", [(5, None), (8, None), (10, 6), (11, 7), (12, 8)])
-def test_plan_replay_matches_oracle(lib, orc, n, tile_bits):
+@pytest.mark.parametrize("fold,tensor", [(0, 0), (0, -1), (-1, -1), (1, -1), (400, -1)])
+@pytest.mark.parametrize("n,tile_bits", [(5, None), (8, None), (10, 6), (11, 7), (12, 8),
+                                         (12, None), (14, None)])
+def test_plan_replay_matches_oracle(lib, orc, n, tile_bits, fold, tensor):
     rng = W.rng_for(1000 + n)
     ops = random_ops(rng, n, 60)
     ops.append(W.Op(random_unitary(rng, 4), [0, n - 1, 2, n - 2]))  # generic step
     ops += random_ops(rng, n, 20)
     psi0 = np.zeros(1 << n, dtype=np.complex128)
     psi0[0] = 1
-    got, steps = run_plan(lib, ops, n, psi0, tile_bits=tile_bits)
+    got, steps = run_plan(lib, ops, n, psi0, tile_bits=tile_bits, fold=fold, tensor=tensor)
     want = oracle_run(orc, ops, n)
     assert np.allclose(got / np.linalg.norm(got), want / np.linalg.norm(want), atol=1e-12)
     assert any(s[0] == 2 for s in steps)
@@ -257,12 +275,17 @@ def test_plan_unfused_one_gate_per_sweep(lib, orc):
 def test_plan_scale_circuit_fusion_ratio(lib):
     """At 30 qubits the depth-40 workload fuses into ~2 sweeps per layer."""
     c = W.scale_circuit(seed=2, n=30, depth=40)
-    steps, blob = build_plan(lib, c.ops, 30)
+    steps, blob = build_plan(lib, c.ops, 30, fold=-1, tensor=-1)
     nsweeps = sum(1 for s in steps if s[0] == 1)
     assert all(s[0] == 1 for s in steps)
     assert nsweeps <= 3 * c.depth
     tot = sum(int(np.frombuffer(blob, HDR, 1, off)[0]["ngate"]) for _, off, _ in steps)
     assert tot == len(c.ops)
+    # pass folding keeps the sweeps and shortens their gate lists
+    fsteps, fblob = build_plan(lib, c.ops, 30, tensor=-1)
+    assert len(fsteps) == len(steps)
+    ftot = sum(int(np.frombuffer(fblob, HDR, 1, off)[0]["ngate"]) for _, off, _ in fsteps)
+    assert ftot < 0.75 * tot
 
 
 def swizzle(i, sw):
@@ -306,3 +329,94 @@ def test_pass_tables_address_every_slot_once(lib, prec, n):
                     raws.append(rw)
             assert sorted(slots) == list(range(1 << m))
             assert sorted(raws) == list(range(1 << m))
+
+
+def warp_slots(p, m, w):
+    """Raw tile indices the threads of warp `w` address in pass `p`."""
+    nthreads = 1 << (m - 3)
+    out = set()
+    for tid in range(32 * w, min(32 * (w + 1), nthreads)):
+        rg = int(p["rlo"][tid & 31]) | int(p["rhi"][tid >> 5])
+        for r in range(8):
+            rw = rg
+            for j in range(3):
+                if (r >> j) & 1:
+                    rw |= int(p["pm"][j])
+            out.add(rw)
+    return out
+
+
+@pytest.mark.parametrize("prec,n,tile_bits", [(2, 14, None), (1, 16, None), (2, 12, 8),
+                                              (2, 16, 12), (2, 10, 7)])
+def test_warp_phases_stay_inside_warps(lib, prec, n, tile_bits):
+    """A pass flagged for a warp barrier only (DK_PASS_WARP) must leave every
+    warp on the same tile slots in the next pass; the last pass of a sweep
+    always ends with a block barrier, and tiles narrower than a warp never
+    use the flag."""
+    ops = random_ops(W.rng_for(500 + n), n, 60)
+    ops += W.scale_circuit(seed=3, n=n, depth=3).ops
+    steps, blob = build_plan(lib, ops, n, prec=prec, tile_bits=tile_bits)
+    flagged = 0
+    for kind, off, _ in steps:
+        if kind != 1:
+            continue
+        h = np.frombuffer(blob, HDR, 1, off)[0]
+        m = int(h["m"])
+        passes = np.frombuffer(blob, PASS, int(h["npass"]), off + int(h["pass_off"]))
+        assert not int(passes[-1]["flags"]) & 2
+        for i in range(len(passes) - 1):
+            if not int(passes[i]["flags"]) & 2:
+                continue
+            assert m >= 8
+            flagged += 1
+            for w in range(max(1, (1 << (m - 3)) // 32)):
+                assert warp_slots(passes[i], m, w) == warp_slots(passes[i + 1], m, w)
+    if (tile_bits or 11) >= 8:
+        assert flagged > 0
+    else:
+        assert flagged == 0
+
+
+def test_scale_circuit_phases_cut_block_barriers(lib):
+    """On the 30-qubit workload most passes end with a warp barrier only."""
+    c = W.scale_circuit(seed=2, n=30, depth=8)
+    steps, blob = build_plan(lib, c.ops, 30)
+    npass = nwarp = 0
+    for kind, off, _ in steps:
+        h = np.frombuffer(blob, HDR, 1, off)[0]
+        passes = np.frombuffer(blob, PASS, int(h["npass"]), off + int(h["pass_off"]))
+        npass += len(passes)
+        nwarp += sum(1 for p in passes if int(p["flags"]) & 2)
+    assert nwarp >= npass // 3, (nwarp, npass)
+
+
+def test_tensor_variants_fold_out_of_tile_conditions(lib, orc):
+    """Tensor sweeps fold gates whose controls lie outside the tile into the
+    pass matrix, one product per combination of the run's tile conditions;
+    the replay of those variant entries equals gate-by-gate application."""
+    n = 15
+    rng = W.rng_for(77)
+    ops = []
+    for layer in range(4):
+        for q in range(n):
+            ops.append(W.Op(W.u3(*rng.uniform(0, 2 * np.pi, 3)), [q]))
+        for q in range(layer % 2, n - 1, 2):
+            ops.append(W.Op(W.X.copy(), [q], {q + 1}))
+        # far controls / anticontrols on low targets
+        for q in range(3):
+            ops.append(W.Op(W.u3(*rng.uniform(0, 2 * np.pi, 3)), [q], {n - 1 - q}, {n - 4 - q}))
+    psi0 = np.zeros(1 << n, dtype=np.complex128)
+    psi0[0] = 1
+    got, steps = run_plan(lib, ops, n, psi0)
+    want = oracle_run(orc, ops, n)
+    assert np.allclose(got / np.linalg.norm(got), want / np.linalg.norm(want), atol=1e-12)
+    _, blob = build_plan(lib, ops, n)
+    nvar = 0
+    for kind, off, _ in steps:
+        if kind != 1:
+            continue
+        h = np.frombuffer(blob, HDR, 1, off)[0]
+        assert int(h["mode"]) == 1
+        g = np.frombuffer(blob, GATE, int(h["ngate"]), off + int(h["gate_off"]))
+        nvar += int((g["code"] == 45).sum())
+    assert nvar > 0

@@ -246,6 +246,12 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 
 /* ---- tensor-core sweep --------------------------------------------------- */
 
+#ifndef DK_TC_SHAPE
+#define DK_TC_SHAPE 4
+#endif
+#ifndef DK_TC_NBUF
+#define DK_TC_NBUF 1
+#endif
 #ifndef DK_TC_MINB11
 #define DK_TC_MINB11 3
 #endif
@@ -263,6 +269,18 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 	    : "d"(a), "d"(b));
 }
 
+/* FP64 tensor-core MMA, D (16x8) += A (16x16, row-major) * B (16x8,
+ * column-major), with g = l/4, t = l%4: lane l holds A[g + 8(i%2)][t + 4(i/2)]
+ * (i < 8), B[t + 4i][g] (i < 4) and D[g + 8(i/2)][2t + i%2] (i < 4). */
+__device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], const double (&b)[4])
+{
+	asm("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, "
+	    "{%4, %5, %6, %7, %8, %9, %10, %11}, {%12, %13, %14, %15}, {%0, %1, %2, %3};\n"
+	    : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+	    : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]),
+	      "d"(a[7]), "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 /* Sweep whose gate list holds only 8x8 matrices in register order (folded
  * runs of gates, and single gates whose remaining controls lie off the pass
  * bits or outside the tile).  A pass works on columns: the 8 amplitudes that
@@ -275,7 +293,7 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
  * and writes amplitude l/4 of columns 2(l%4) and 2(l%4)+1.  Entries with
  * controls off the pass bits write only the columns whose tile index
  * satisfies them; the others keep their values in the shared tile. */
-template <typename R, int SW, int M, int MINB>
+template <typename R, int SW, int M, int MINB, int NBUF>
 __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 	k_sweep_tc(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
 		   const unsigned char *__restrict__ prog, double *partials)
@@ -290,8 +308,8 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 	const uint32_t tn_amp = 1u << m;
 	const int ncond = (int)h->ncond;
 	const size_t gate_bytes = (size_t)ngate * sizeof(dk_gate_desc);
-	C2 *tile = reinterpret_cast<C2 *>(sm);
-	uint4 *sg = reinterpret_cast<uint4 *>(sm + sizeof(C2) * tn_amp);
+	C2 *const bufs = reinterpret_cast<C2 *>(sm);
+	uint4 *sg = reinterpret_cast<uint4 *>(sm + NBUF * sizeof(C2) * tn_amp);
 	dk_gate_cond *scond =
 		reinterpret_cast<dk_gate_cond *>(reinterpret_cast<unsigned char *>(sg) + gate_bytes);
 	const dk_pass_desc *passes = reinterpret_cast<const dk_pass_desc *>(prog + h->pass_off);
@@ -363,11 +381,11 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		}
 		return ntiles;
 	};
-	auto prefetch = [&](uint64_t base) {
+	auto prefetch = [&](uint64_t base, C2 *buf) {
 		const uint64_t bo = base | off_t;
 #pragma unroll
 		for (int r = 0; r < NA; ++r) {
-			C2 *dst = tile + (stid ^ sro[r]);
+			C2 *dst = buf + (stid ^ sro[r]);
 			if (sizeof(C2) == 16)
 				cp_async16(dst, in + (bo | soff[r]));
 			else
@@ -379,11 +397,25 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 	double insq = 0.0, outsq = 0.0;
 	uint64_t t = next_tile(blockIdx.x);
 	if (t < ntiles)
-		prefetch(tile_base(t));
+		prefetch(tile_base(t), bufs);
 	const uint32_t gl = lane >> 2, gk = lane & 3u;
+	int cur = 0;
 	while (t < ntiles) {
 		const uint64_t base = tile_base(t);
-		cp_async_wait_all();
+		C2 *const tile = bufs + (NBUF == 2 ? cur * tn_amp : 0);
+		uint64_t tn = ntiles;
+		if (NBUF == 2) {
+			/* the next tile streams into the other buffer meanwhile */
+			tn = next_tile(t + gridDim.x);
+			if (tn < ntiles) {
+				prefetch(tile_base(tn), bufs + (cur ^ 1) * tn_amp);
+				asm volatile("cp.async.wait_group 1;\n" ::);
+			} else {
+				cp_async_wait_all();
+			}
+		} else {
+			cp_async_wait_all();
+		}
 		__syncthreads();
 		if (skip_idle) {
 			/* only touched tiles reach here: their old |amp|^2 leaves csq */
@@ -393,7 +425,12 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		}
 		for (int p = 0; p < npass; ++p) {
 			const dk_pass_desc *pd = passes + p;
+			/* the slot tables are XOR-linear in the thread index: a column's
+			 * slot is the XOR of the entries of its set bits */
 			const uint32_t shw = __ldg(&pd->shi[warp]);
+			const uint32_t t8 = __ldg(&pd->slo[8]), t16 = __ldg(&pd->slo[16]);
+			const uint32_t sgl = __ldg(&pd->slo[gl]) ^ shw;
+			const uint32_t sgk = __ldg(&pd->slo[2u * gk]) ^ shw, t1 = __ldg(&pd->slo[1]);
 			const uint32_t s0 = __ldg(&pd->sp[0]), s1 = __ldg(&pd->sp[1]),
 				       s2 = __ldg(&pd->sp[2]);
 			const uint32_t gj0 = ((gk & 1u) ? s0 : 0u) ^ ((gk & 2u) ? s1 : 0u);
@@ -422,49 +459,49 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 				}
 				const double2 *mt = mats + 64 * (size_t)mi + 8 * gl + gk;
 				const double2 e0 = __ldg(mt), e1 = __ldg(mt + 4);
+#if DK_TC_SHAPE == 16
+				const double wa[8] = { e0.x, e0.y, e1.x, e1.y, -e0.y, e0.x, -e1.y, e1.x };
+#endif
 				const bool ctl = code == DK_GC_DENSE3 + 1;
-				/* two column groups at a time: their slots are disjoint
-				 * from the other groups' */
+				/* one column group at a time: the groups' slots are
+				 * disjoint */
 #pragma unroll
-				for (int q0 = 0; q0 < 4; q0 += 2) {
-					double y[2][4];
+				for (int q = 0; q < 4; ++q) {
+					const uint32_t bg = sgl ^ ((q & 1) ? t8 : 0u) ^ ((q & 2) ? t16 : 0u);
+					const double2 x0 = to_c128(tile[bg ^ gj0]);
+					const double2 x1 = to_c128(tile[bg ^ gj1]);
+					double y[4] = { 0.0, 0.0, 0.0, 0.0 };
+#if DK_TC_SHAPE == 16
+					dmma16(y, wa, { x0.x, x1.x, x0.y, x1.y });
+#else
+					/* Gauss: Mr xr, Mi xi and (Mr + Mi)(xr + xi), three real
+					 * 8x8 products of two k-steps each */
+					double p1[2] = { 0.0, 0.0 }, p2[2] = { 0.0, 0.0 }, p3[2] = { 0.0, 0.0 };
+					dmma(p1[0], p1[1], e0.x, x0.x);
+					dmma(p2[0], p2[1], e0.y, x0.y);
+					dmma(p3[0], p3[1], e0.x + e0.y, x0.x + x0.y);
+					dmma(p1[0], p1[1], e1.x, x1.x);
+					dmma(p2[0], p2[1], e1.y, x1.y);
+					dmma(p3[0], p3[1], e1.x + e1.y, x1.x + x1.y);
+					y[0] = p1[0] - p2[0];
+					y[1] = p1[1] - p2[1];
+					y[2] = p3[0] - p1[0] - p2[0];
+					y[3] = p3[1] - p1[1] - p2[1];
+#endif
+					__syncwarp(); /* the group's gathers precede its writes */
 #pragma unroll
-					for (int h2 = 0; h2 < 2; ++h2) {
-						const int q = q0 + h2;
-						const uint32_t bg = __ldg(&pd->slo[(q << 3) | gl]) ^ shw;
-						const double2 x0 = to_c128(tile[bg ^ gj0]);
-						const double2 x1 = to_c128(tile[bg ^ gj1]);
-						double r0 = 0.0, r1 = 0.0, i0 = 0.0, i1 = 0.0;
-						dmma(r0, r1, e0.x, x0.x);
-						dmma(i0, i1, e0.y, x0.x);
-						dmma(r0, r1, e1.x, x1.x);
-						dmma(i0, i1, e1.y, x1.x);
-						dmma(r0, r1, -e0.y, x0.y);
-						dmma(i0, i1, e0.x, x0.y);
-						dmma(r0, r1, -e1.y, x1.y);
-						dmma(i0, i1, e1.x, x1.y);
-						y[h2][0] = r0;
-						y[h2][1] = r1;
-						y[h2][2] = i0;
-						y[h2][3] = i1;
-					}
-					__syncwarp(); /* the groups' gathers precede their writes */
-#pragma unroll
-					for (int h2 = 0; h2 < 2; ++h2)
-#pragma unroll
-						for (int e = 0; e < 2; ++e) {
-							const uint32_t col =
-								((q0 + h2) << 3) | (2u * gk + e);
-							if (ctl) {
-								const uint32_t raw = __ldg(&pd->rlo[col]) |
-										     __ldg(&pd->rhi[warp]);
-								if (!ctl_ok(raw, d.z, d.w))
-									continue;
-							}
-							const uint32_t bs = __ldg(&pd->slo[col]) ^ shw;
-							tile[bs ^ sr] = from_c128<C2>(
-								make_double2(y[h2][e], y[h2][2 + e]));
+					for (int e = 0; e < 2; ++e) {
+						if (ctl) { /* rare: controls off the pass bits */
+							const uint32_t col = (q << 3) | (2u * gk + e);
+							const uint32_t raw = __ldg(&pd->rlo[col]) |
+									     __ldg(&pd->rhi[warp]);
+							if (!ctl_ok(raw, d.z, d.w))
+								continue;
 						}
+						const uint32_t bs = sgk ^ (e ? t1 : 0u) ^ ((q & 1) ? t8 : 0u) ^
+								    ((q & 2) ? t16 : 0u);
+						tile[bs ^ sr] = from_c128<C2>(make_double2(y[e], y[2 + e]));
+					}
 				}
 				__syncwarp();
 			}
@@ -475,10 +512,12 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 #pragma unroll
 		for (int r = 0; r < NA; ++r)
 			a[r] = tile[stid ^ sro[r]];
-		__syncthreads(); /* the buffer is free: start the next tile's copy */
-		const uint64_t tn = next_tile(t + gridDim.x);
-		if (tn < ntiles)
-			prefetch(tile_base(tn));
+		__syncthreads(); /* the buffer is free */
+		if (NBUF == 1) {
+			tn = next_tile(t + gridDim.x);
+			if (tn < ntiles)
+				prefetch(tile_base(tn), bufs);
+		}
 		const uint64_t bo = base | off_t;
 #pragma unroll
 		for (int r = 0; r < NA; ++r) {
@@ -486,6 +525,7 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 			__stcs(out + (bo | soff[r]), a[r]);
 		}
 		t = tn;
+		cur ^= 1;
 	}
 	cp_async_wait_all();
 	block_sum2(insq, outsq);
@@ -991,16 +1031,16 @@ static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dpr
 	return cudaGetLastError();
 }
 
-template <typename R, int SW, int M, int MINB>
+template <typename R, int SW, int M, int MINB, int NBUF>
 static cudaError_t run_sweep_tc(const void *in, void *out, const unsigned char *dprog,
 				const dk_sweep_hdr *hp, int num_sms, const Scratch &s,
 				cudaStream_t st, int *blocks_out)
 {
 	typedef typename CT<R>::T C2;
 	const int m = hp->m;
-	const size_t smem = (sizeof(C2) << m) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
+	const size_t smem = NBUF * (sizeof(C2) << m) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
 			    (size_t)hp->ncond * sizeof(dk_gate_cond);
-	auto kern = k_sweep_tc<R, SW, M, MINB>;
+	auto kern = k_sweep_tc<R, SW, M, MINB, NBUF>;
 	/* raised once to the device maximum, never lowered (see run_sweep) */
 	static std::once_flag once;
 	static cudaError_t set_err = cudaSuccess;
@@ -1042,14 +1082,14 @@ cudaError_t launch_sweep(int prec, const void *in, void *out,
 	if (hp->mode == DK_SWEEP_TENSOR) {
 		/* FP64 tensor-core passes; tiles of 8 to 12 bits */
 		if (prec == DK_C128)
-			e = m >= 12 ? run_sweep_tc<double, 3, 12, DK_TC_MINB12>(in, out, dprog, hp,
+			e = m >= 12 ? run_sweep_tc<double, 3, 12, DK_TC_MINB12, 1>(in, out, dprog, hp,
 										num_sms, s, st, &blocks)
-				    : run_sweep_tc<double, 3, 11, DK_TC_MINB11>(in, out, dprog, hp,
+				    : run_sweep_tc<double, 3, 11, DK_TC_MINB11, DK_TC_NBUF>(in, out, dprog, hp,
 										num_sms, s, st, &blocks);
 		else
-			e = m >= 12 ? run_sweep_tc<float, 4, 12, DK_TC_MINB12>(in, out, dprog, hp,
+			e = m >= 12 ? run_sweep_tc<float, 4, 12, DK_TC_MINB12, 1>(in, out, dprog, hp,
 									       num_sms, s, st, &blocks)
-				    : run_sweep_tc<float, 4, 11, DK_TC_MINB11>(in, out, dprog, hp,
+				    : run_sweep_tc<float, 4, 11, DK_TC_MINB11, DK_TC_NBUF>(in, out, dprog, hp,
 									       num_sms, s, st, &blocks);
 		if (e != cudaSuccess)
 			return e;

@@ -226,6 +226,66 @@ static int phase_score(const uint32_t *pmask, int cnt, uint32_t W, int m, int re
 	return score;
 }
 
+/* Tensor sweeps read and write a pass's columns in two patterns: a gather
+ * whose quarter-warp (16-byte amplitudes) or half-warp (8-byte) varies thread
+ * bit 0 (and 1 for 8-byte) with pass bits 0 and 1, and a scatter that varies
+ * pass bit 0 (and 1) with thread bits 1 and 2.  Under the XOR swizzle each
+ * tile bit b moves the bank group by the unit vector of b mod res, so a phase
+ * takes 2^(varying bits - distinct residues) wavefronts. */
+static int nres(const int *b, int cnt, int res)
+{
+	unsigned seen = 0;
+	for (int i = 0; i < cnt; i++)
+		seen |= 1u << (b[i] % res);
+	return popc(seen);
+}
+
+static int tc_cost(int pb0, int pb1, int l0, int l1, int l2, int res)
+{
+	if (res == 3) {
+		const int g[3] = { l0, pb0, pb1 }, t[3] = { pb0, l1, l2 };
+		return (1 << (3 - nres(g, 3, 3))) + (1 << (3 - nres(t, 3, 3)));
+	}
+	const int g[4] = { l0, l1, pb0, pb1 }, t[4] = { pb0, pb1, l1, l2 };
+	return (1 << (4 - nres(g, 4, res))) + (1 << (4 - nres(t, 4, res)));
+}
+
+/* Cheapest order of pass bits P (register bits 0..2) and choice of thread
+ * bits 0..2 among the lane bits L; returns the cost. */
+static int tc_best(uint32_t P, uint32_t L, int m, int res, uint8_t *pb, uint8_t *l3)
+{
+	int p[DK_PASS_BITS], np = 0, l[32], nl = 0, best = 1 << 30;
+	for (int b = 0; b < m; b++) {
+		if (P >> b & 1u)
+			p[np++] = b;
+		else if (L >> b & 1u)
+			l[nl++] = b;
+	}
+	static const int perm[6][3] = { { 0, 1, 2 }, { 0, 2, 1 }, { 1, 0, 2 },
+					{ 1, 2, 0 }, { 2, 0, 1 }, { 2, 1, 0 } };
+	for (int o = 0; o < 6; o++)
+		for (int a = 0; a < nl; a++)
+			for (int b2 = 0; b2 < nl; b2++)
+				for (int c = 0; c < nl; c++) {
+					if (a == b2 || a == c || b2 == c)
+						continue;
+					const int cost = tc_cost(p[perm[o][0]], p[perm[o][1]], l[a],
+								 l[b2], l[c], res);
+					if (cost < best) {
+						best = cost;
+						if (pb)
+							for (int j = 0; j < 3; j++)
+								pb[j] = (uint8_t)p[perm[o][j]];
+						if (l3) {
+							l3[0] = (uint8_t)l[a];
+							l3[1] = (uint8_t)l[b2];
+							l3[2] = (uint8_t)l[c];
+						}
+					}
+				}
+	return best;
+}
+
 /* A phase: consecutive passes [0, cnt) whose pass bits all avoid the same
  * `wbits` tile bits W, which every pass maps to the thread bits above the 5
  * lane bits.  A warp then touches the same tile slots in every pass of the
@@ -233,7 +293,7 @@ static int phase_score(const uint32_t *pmask, int cnt, uint32_t W, int m, int re
  * target bits of pass i; they are filled up to DK_PASS_BITS from the phase's
  * union first (keeping it small), W is picked from the rest. */
 static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, int wbits,
-			int res, uint8_t (*pbits)[DK_PASS_BITS])
+			int res, int tensor, uint8_t (*pbits)[DK_PASS_BITS])
 {
 	uint32_t F = 0, pmask[64];
 	for (int i = 0; i < cnt; i++)
@@ -255,17 +315,47 @@ static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, 
 	 * conflict free (first one found on ties) */
 	const uint32_t pool = ((1u << m) - 1u) & ~F;
 	uint32_t W = 0;
-	int best = -1;
+	int best = 0, have = 0;
 	for (uint32_t x = pool;; x = (x - 1) & pool) {
 		if (popc(x) == wbits) {
-			const int sc = phase_score(pmask, cnt, x, m, res);
-			if (sc > best) {
+			int sc;
+			if (tensor) {
+				/* fewest shared-memory wavefronts of the tensor passes */
+				sc = 0;
+				for (int i = 0; i < cnt; i++)
+					sc -= tc_best(pmask[i], ((1u << m) - 1u) & ~pmask[i] & ~x, m,
+						      res, NULL, NULL);
+			} else {
+				sc = phase_score(pmask, cnt, x, m, res);
+			}
+			if (!have || sc > best) {
 				best = sc;
 				W = x;
+				have = 1;
 			}
 		}
 		if (x == 0)
 			break;
+	}
+	if (tensor) {
+		for (int i = 0; i < cnt; i++) {
+			uint8_t lane[32], l3[3];
+			const uint32_t L = ((1u << m) - 1u) & ~pmask[i] & ~W;
+			tc_best(pmask[i], L, m, res, pbits[i], l3);
+			int nl = 0;
+			for (int j = 0; j < 3; j++)
+				lane[nl++] = l3[j];
+			for (int b = 0; b < m; b++)
+				if ((L >> b & 1u) && b != l3[0] && b != l3[1] && b != l3[2])
+					lane[nl++] = (uint8_t)b;
+			for (int b = 0; b < m; b++)
+				if (W & (1u << b))
+					lane[nl++] = (uint8_t)b;
+			pass_tables_lanes(&pd[i], pbits[i], lane, nl, res);
+			if (i + 1 < cnt)
+				pd[i].flags |= DK_PASS_WARP;
+		}
+		return;
 	}
 	for (int i = 0; i < cnt; i++) {
 		uint8_t lane[32], free_bits[32];
@@ -569,7 +659,8 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 			uint32_t U = need[p0];
 			while (p1 < npass && p1 - p0 < 64 && popc(U | need[p1]) <= m - wbits)
 				U |= need[p1++];
-			build_phase(&passes[p0], &need[p0], p1 - p0, m, wbits, res, &pbits[p0]);
+			build_phase(&passes[p0], &need[p0], p1 - p0, m, wbits, res, fold->tensor,
+				    &pbits[p0]);
 		} else {
 			uint32_t P = need[p0];
 			for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)

@@ -259,7 +259,8 @@ def engine_arm(args, rank, world, local_rank):
         "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(n, depth, c),
-        "roofline": {"bound": "hbm", "kernel": "k_sweep<double> (fused gate sweep)",
+        "roofline": {"bound": "hbm",
+                     "kernel": "k_sweep_tc<double> (fused gate sweep, FP64 tensor-core passes)",
                      "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind + " hbm_gbs (copy)", "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,

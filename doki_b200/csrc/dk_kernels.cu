@@ -418,10 +418,13 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		}
 		__syncthreads();
 		if (skip_idle) {
-			/* only touched tiles reach here: their old |amp|^2 leaves csq */
+			/* only touched tiles reach here: their old |amp|^2 leaves csq.
+			 * The read uses the identity mapping, so every thread must be
+			 * done with it before the first pass writes the tile. */
 #pragma unroll
 			for (int r = 0; r < NA; ++r)
 				insq += sqabs(tile[stid ^ sro[r]]);
+			__syncthreads();
 		}
 		for (int p = 0; p < npass; ++p) {
 			const dk_pass_desc *pd = passes + p;

@@ -197,6 +197,32 @@ def test_fused_equals_unfused(dk_gpu, orc, fuse):
     assert np.allclose(got, orc.registry_get_all(b), atol=ATOL_C128, rtol=0)
 
 
+@pytest.mark.parametrize("n", [22, 23])
+def test_conditioned_in_place_sweeps_keep_the_norm(dk_gpu, orc, n):
+    """Sweeps whose gates all depend on one qubit outside the tile skip the
+    tiles where it is 0 and update the stored norm from the touched tiles
+    only; repeated many times, the normalised state must keep unit norm and
+    equal the oracle."""
+    d = dk_gpu
+    rng = W.rng_for(900 + n)
+    ops = [W.Op(W.u3(*rng.uniform(0, 2 * np.pi, 3)), [q]) for q in range(n)]
+    reg = W.run_ops(d, d.registry_new(n, False), ops)
+    d.registry_flush(reg)
+    c = n - 1  # far control: outside every tile
+    for rnd in range(24):
+        batch = []
+        for j in range(6):
+            m = W.u3(*rng.uniform(0, 2 * np.pi, 3))
+            batch.append(W.Op(m, [(rnd + j) % 6], {c} if rnd % 3 else set(), set() if rnd % 3 else {c}))
+        reg = W.run_ops(d, reg, batch)
+        d.registry_flush(reg)
+        amps = allamps(d, reg)
+        assert abs(float(np.sum(np.abs(amps) ** 2)) - 1.0) < 1e-12, rnd
+        ops += batch
+    want = W.run_ops(orc, orc.registry_new(n), ops)
+    assert np.allclose(amps, orc.registry_get_all(want), atol=ATOL_C128, rtol=0)
+
+
 def test_copy_on_write_semantics(dk_gpu):
     """Every operation returns a new register; inputs are never mutated."""
     d = dk_gpu

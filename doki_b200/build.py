@@ -87,7 +87,7 @@ def build(force: bool = False, verbose: bool = False) -> None:
                   "-c", s, "-o", o])
         objs.append(o)
     if force or _stale(LIB, objs):
-        _run([nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcublas",
+        _run([nvcc, *ARCH, "-shared", "-o", LIB, *objs,
               "-Xlinker", "-rpath=/usr/local/cuda/lib64"])
     msrc = os.path.join(CSRC, "doki_module.c")
     if force or _stale(EXT, [msrc, LIB, os.path.join(INC, "dokigpu.h")]):

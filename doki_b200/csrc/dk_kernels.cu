@@ -875,6 +875,192 @@ __global__ void __launch_bounds__(256)
 	}
 }
 
+/* ---- reduced density matrix -------------------------------------------
+ * rho = alpha X X^H, X[a][b] = A[b * dim + a] (a: kept index, b: traced
+ * index), into the lower triangle of the column-major C (C[a + a' dim],
+ * a >= a').  The traced index is split into nsplit chunks whose partial
+ * products go to part[s] and are added in a fixed order by k_rho_reduce. */
+
+constexpr int kRhoTile = 64; /* output tile (rows and columns) */
+constexpr int kRhoSlab = 16; /* traced values per shared-memory slab */
+
+__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, bool valid)
+{
+	const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem),
+		     "r"(valid ? 16 : 0));
+}
+
+/* One lower 64x64 tile (ti >= tj) per CTA and one traced chunk per grid row.
+ * 8 warps as 2 x 4: a warp owns rows 32 wr .. +32 (4 MMA row blocks) and
+ * columns 16 wc .. +16 (2 column blocks).  Per 4 traced values (one k-step)
+ * each 8x8 block takes 4 FP64 MMAs:
+ *   re += Xr Xr'^T + Xi Xi'^T,  im += Xi Xr'^T - Xr Xi'^T.
+ * Slabs are stored [b][a ^ 2 (b & 3)] so a quarter-warp's fragment reads
+ * (4 traced rows x 2 columns) hit 8 distinct 16-byte bank groups. */
+__global__ void __launch_bounds__(256, 2)
+	k_rho_tc(const double2 *__restrict__ A, uint64_t dim, uint64_t K, uint64_t bchunk,
+		 double2 *part, double alpha)
+{
+	extern __shared__ __align__(16) unsigned char rsm[];
+	/* [buffer][row tile, column tile][traced][kept] */
+	double2 (*sab)[2][kRhoSlab][kRhoTile] =
+		reinterpret_cast<double2 (*)[2][kRhoSlab][kRhoTile]>(rsm);
+	const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+	const uint32_t g = lane >> 2, t = lane & 3u, wr = warp & 1u, wc = warp >> 1;
+	/* lower-triangle tile index -> (ti, tj) */
+	const uint64_t x = blockIdx.x;
+	uint64_t ti = (uint64_t)((sqrt(8.0 * (double)x + 1.0) - 1.0) * 0.5);
+	while ((ti + 1) * (ti + 2) / 2 <= x)
+		++ti;
+	while (ti * (ti + 1) / 2 > x)
+		--ti;
+	const uint64_t tj = x - ti * (ti + 1) / 2;
+	const uint64_t a0 = ti * kRhoTile, c0 = tj * kRhoTile;
+	const bool diag = ti == tj;
+	const uint64_t b_begin = (uint64_t)blockIdx.y * bchunk;
+	uint64_t b_end = b_begin + bchunk;
+	if (b_end > K)
+		b_end = K;
+
+	auto load = [&](int buf, uint64_t b0) {
+#pragma unroll
+		for (int r = 0; r < (kRhoSlab * kRhoTile) / 256; ++r) {
+			const uint32_t e = tid + 256u * r;
+			const uint32_t bl = e / kRhoTile, al = e % kRhoTile;
+			const uint64_t b = b0 + bl;
+			const bool ok = b < b_end;
+			const uint32_t pa = al ^ ((bl & 3u) << 1);
+			cp_async16_zfill(&sab[buf][0][bl][pa], A + (ok ? b * dim + a0 + al : 0), ok);
+			if (!diag)
+				cp_async16_zfill(&sab[buf][1][bl][pa], A + (ok ? b * dim + c0 + al : 0),
+						 ok);
+		}
+		cp_async_commit();
+	};
+
+	double acc[4][2][4];
+#pragma unroll
+	for (int i = 0; i < 4; ++i)
+#pragma unroll
+		for (int j = 0; j < 2; ++j)
+#pragma unroll
+			for (int v = 0; v < 4; ++v)
+				acc[i][j][v] = 0.0;
+
+	const int bsel = diag ? 0 : 1;
+	int cur = 0;
+	if (b_begin < b_end)
+		load(0, b_begin);
+	for (uint64_t b0 = b_begin; b0 < b_end; b0 += kRhoSlab) {
+		if (b0 + kRhoSlab < b_end) {
+			load(cur ^ 1, b0 + kRhoSlab);
+			asm volatile("cp.async.wait_group 1;\n" ::);
+		} else {
+			cp_async_wait_all();
+		}
+		__syncthreads();
+#pragma unroll
+		for (int ks = 0; ks < kRhoSlab / 4; ++ks) {
+			const uint32_t bl = 4u * ks + t;
+			const uint32_t sw = (bl & 3u) << 1;
+			double2 xa[4], xb[2];
+#pragma unroll
+			for (int i = 0; i < 4; ++i)
+				xa[i] = sab[cur][0][bl][(32u * wr + 8u * i + g) ^ sw];
+#pragma unroll
+			for (int j = 0; j < 2; ++j)
+				xb[j] = sab[cur][bsel][bl][(16u * wc + 8u * j + g) ^ sw];
+#pragma unroll
+			for (int i = 0; i < 4; ++i)
+#pragma unroll
+				for (int j = 0; j < 2; ++j) {
+					dmma(acc[i][j][0], acc[i][j][1], xa[i].x, xb[j].x);
+					dmma(acc[i][j][0], acc[i][j][1], xa[i].y, xb[j].y);
+					dmma(acc[i][j][2], acc[i][j][3], xa[i].y, xb[j].x);
+					dmma(acc[i][j][2], acc[i][j][3], -xa[i].x, xb[j].y);
+				}
+		}
+		__syncthreads(); /* this buffer is refilled two slabs later */
+		cur ^= 1;
+	}
+	double2 *P = part + (uint64_t)blockIdx.y * dim * dim;
+	const double f = gridDim.y == 1 ? alpha : 1.0;
+#pragma unroll
+	for (int i = 0; i < 4; ++i)
+#pragma unroll
+		for (int j = 0; j < 2; ++j)
+#pragma unroll
+			for (int e = 0; e < 2; ++e) {
+				const uint64_t a = a0 + 32u * wr + 8u * i + g;
+				const uint64_t c = c0 + 16u * wc + 8u * j + 2u * t + e;
+				P[a + c * dim] = make_double2(f * acc[i][j][e], f * acc[i][j][2 + e]);
+			}
+}
+
+/* Kept sets below 64 amplitudes: one CTA per traced chunk stages the chunk
+ * and every thread accumulates up to 4 of the dim^2 products. */
+__global__ void __launch_bounds__(256)
+	k_rho_small(const double2 *__restrict__ A, uint32_t dim, uint64_t K, uint64_t bchunk,
+		    double2 *part)
+{
+	__shared__ double2 sx[2048];
+	const uint32_t per = 2048u / dim; /* traced values per staging round */
+	const uint64_t b_begin = (uint64_t)blockIdx.x * bchunk;
+	uint64_t b_end = b_begin + bchunk;
+	if (b_end > K)
+		b_end = K;
+	double re[4] = { 0.0, 0.0, 0.0, 0.0 }, im[4] = { 0.0, 0.0, 0.0, 0.0 };
+	const uint32_t nout = dim * dim;
+	for (uint64_t b0 = b_begin; b0 < b_end; b0 += per) {
+		const uint64_t nb = (b_end - b0) < per ? (b_end - b0) : per;
+		for (uint32_t e = threadIdx.x; e < nb * dim; e += blockDim.x)
+			sx[e] = A[b0 * dim + e];
+		__syncthreads();
+#pragma unroll
+		for (int r = 0; r < 4; ++r) {
+			const uint32_t o = threadIdx.x + 256u * r;
+			if (o >= nout)
+				continue;
+			const uint32_t a = o % dim, c = o / dim;
+			for (uint32_t b = 0; b < nb; ++b) {
+				const double2 u = sx[b * dim + a], v = sx[b * dim + c];
+				re[r] = fma(u.x, v.x, fma(u.y, v.y, re[r]));
+				im[r] = fma(u.y, v.x, fma(-u.x, v.y, im[r]));
+			}
+		}
+		__syncthreads();
+	}
+	double2 *P = part + (uint64_t)blockIdx.x * nout;
+#pragma unroll
+	for (int r = 0; r < 4; ++r) {
+		const uint32_t o = threadIdx.x + 256u * r;
+		if (o < nout)
+			P[o] = make_double2(re[r], im[r]);
+	}
+}
+
+/* C = alpha * sum over s (in order) of part[s], on the lower tiles */
+__global__ void __launch_bounds__(256)
+	k_rho_reduce(const double2 *__restrict__ part, int nsplit, uint64_t dim, double alpha,
+		     double2 *C)
+{
+	const uint64_t total = dim * dim;
+	for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+	     e += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t a = e % dim, c = e / dim;
+		if (a / kRhoTile < c / kRhoTile)
+			continue;
+		double x = 0.0, y = 0.0;
+		for (int s2 = 0; s2 < nsplit; ++s2) {
+			const double2 v = part[(uint64_t)s2 * total + e];
+			x += v.x;
+			y += v.y;
+		}
+		C[e] = make_double2(alpha * x, alpha * y);
+	}
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256)
 	k_rho_elem(const typename CT<R>::T *__restrict__ d, uint64_t ia, uint64_t ib,
@@ -1332,6 +1518,55 @@ cudaError_t launch_herm_fill(const double2 *C, double2 *rho, uint64_t dim,
 	const int blocks = grid_for(dim * dim, 256 * 4, g_num_sms * 8);
 	k_herm_fill<<<blocks, 256, 0, st>>>(C, rho, dim);
 	g_launches += 1;
+	return cudaGetLastError();
+}
+
+int rho_splits(uint64_t dim, uint64_t K, int num_sms)
+{
+	if (dim < (uint64_t)kRhoTile) {
+		uint64_t ns = (K + 4095) / 4096; /* traced values per small CTA: 4096 */
+		if (ns > 1024)
+			ns = 1024;
+		return ns ? (int)ns : 1;
+	}
+	const uint64_t T = dim / kRhoTile, ntile = T * (T + 1) / 2;
+	uint64_t ns = 1;
+	while (ntile * ns < (uint64_t)num_sms * 4 && ns * 256 <= K && ns < 64)
+		ns *= 2;
+	return (int)ns;
+}
+
+cudaError_t launch_rho(const double2 *A, uint64_t dim, uint64_t K, double alpha, int nsplit,
+		       double2 *part, double2 *C, cudaStream_t st)
+{
+	if (dim < (uint64_t)kRhoTile) {
+		const uint64_t bchunk = (K + nsplit - 1) / nsplit;
+		k_rho_small<<<nsplit, 256, 0, st>>>(A, (uint32_t)dim, K, bchunk, part);
+		const int blocks = grid_for(dim * dim, 256, g_num_sms * 8);
+		k_rho_reduce<<<blocks, 256, 0, st>>>(part, nsplit, dim, alpha, C);
+		g_launches += 2;
+		return cudaGetLastError();
+	}
+	const uint64_t T = dim / kRhoTile, ntile = T * (T + 1) / 2;
+	uint64_t bchunk = (K + nsplit - 1) / nsplit;
+	bchunk = (bchunk + kRhoSlab - 1) / kRhoSlab * kRhoSlab;
+	const size_t smem = sizeof(double2) * 2 * 2 * kRhoSlab * kRhoTile;
+	static std::once_flag once;
+	static cudaError_t set_err = cudaSuccess;
+	std::call_once(once, [&] {
+		set_err = cudaFuncSetAttribute(k_rho_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+					       (int)smem);
+	});
+	if (set_err != cudaSuccess)
+		return set_err;
+	dim3 grid((unsigned)ntile, (unsigned)nsplit);
+	k_rho_tc<<<grid, 256, smem, st>>>(A, dim, K, bchunk, nsplit == 1 ? C : part, alpha);
+	g_launches += 1;
+	if (nsplit > 1) {
+		const int blocks = grid_for(dim * dim, 256 * 4, g_num_sms * 8);
+		k_rho_reduce<<<blocks, 256, 0, st>>>(part, nsplit, dim, alpha, C);
+		g_launches += 1;
+	}
 	return cudaGetLastError();
 }
 

@@ -78,6 +78,13 @@ cudaError_t launch_first_nonzero(int prec, const void *d, uint64_t first,
 cudaError_t launch_gather_kept(int prec, const void *d, unsigned n,
 			       uint64_t keep_mask, double2 *M, cudaStream_t st);
 
+/* rho = alpha X X^H (X[a][b] = A[b * dim + a]) into the lower triangle of
+ * the column-major C; nsplit = rho_splits(...) partials of dim * dim each
+ * in part (unused when nsplit == 1 and dim >= 64) */
+int rho_splits(uint64_t dim, uint64_t K, int num_sms);
+cudaError_t launch_rho(const double2 *A, uint64_t dim, uint64_t K, double alpha, int nsplit,
+		       double2 *part, double2 *C, cudaStream_t st);
+
 /* lower triangle of the column-major Hermitian C -> full row-major rho */
 cudaError_t launch_herm_fill(const double2 *C, double2 *rho, uint64_t dim,
 			     cudaStream_t st);

@@ -11,7 +11,6 @@
  * and every sweep recomputes the norm, the result equals the reference's
  * gate-by-gate renormalised evolution (qops.c:176-261) for any grouping.
  */
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -35,7 +34,6 @@ namespace {
 struct Slot {
 	cudaStream_t st = nullptr;
 	dk::Scratch scratch{};
-	cublasHandle_t blas = nullptr;
 	std::recursive_mutex mu;
 };
 
@@ -1165,13 +1163,6 @@ int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)
 		return DK_ERR_ARG;
 	const uint64_t dim = 1ull << k;
 	const uint64_t K = 1ull << (n - k);
-	if (!CUR.blas) {
-		if (cublasCreate(&CUR.blas) != CUBLAS_STATUS_SUCCESS) {
-			snprintf(g.err, sizeof(g.err), "cublasCreate failed");
-			return DK_ERR_CUDA;
-		}
-		cublasSetStream(CUR.blas, CUR.st);
-	}
 	const bool direct = (s->prec == DK_C128) && (keep_mask == dim - 1);
 	double2 *C = nullptr, *rho = nullptr, *M = nullptr;
 	rc = dev_alloc((void **)&C, 16 * dim * dim);
@@ -1197,32 +1188,33 @@ int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)
 		A = M;
 	}
 	const double alpha = 1.0 / (s->norm * s->norm);
-	const uint64_t chunk = 1ull << 24;
-	cublasStatus_t bs = CUBLAS_STATUS_SUCCESS;
-	for (uint64_t k0 = 0; e == cudaSuccess && k0 < K && bs == CUBLAS_STATUS_SUCCESS;
-	     k0 += chunk) {
-		const uint64_t kc = (K - k0) < chunk ? (K - k0) : chunk;
-		const double beta = k0 ? 1.0 : 0.0;
-		bs = cublasZherk(CUR.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, (int)dim,
-				 (int)kc, &alpha,
-				 (const cuDoubleComplex *)(A + k0 * dim), (int)dim, &beta,
-				 (cuDoubleComplex *)C, (int)dim);
+	/* tensor-core product X X^H, split over the traced index into partials
+	 * that are added in a fixed order */
+	const int ns = dk::rho_splits(dim, K, g.num_sms);
+	double2 *part = nullptr;
+	const size_t pbytes = (ns > 1 || dim < 64) ? 16 * dim * dim * (size_t)ns : 0;
+	if (pbytes && dev_alloc((void **)&part, pbytes) != DK_OK) {
+		dev_free(C, 16 * dim * dim);
+		dev_free(rho, 16 * dim * dim);
+		if (M)
+			dev_free(M, 16ull << n);
+		return DK_ERR_ALLOC;
 	}
-	if (e == cudaSuccess && bs == CUBLAS_STATUS_SUCCESS)
+	if (e == cudaSuccess)
+		e = dk::launch_rho(A, dim, K, alpha, ns, part, C, CUR.st);
+	if (e == cudaSuccess)
 		e = dk::launch_herm_fill(C, rho, dim, CUR.st);
-	if (e == cudaSuccess && bs == CUBLAS_STATUS_SUCCESS)
+	if (e == cudaSuccess)
 		e = cudaMemcpyAsync(out, rho, 16 * dim * dim, cudaMemcpyDeviceToHost, CUR.st);
 	g.d2h += 16 * dim * dim;
 	if (e == cudaSuccess)
 		e = cudaStreamSynchronize(CUR.st);
 	dev_free(C, 16 * dim * dim);
 	dev_free(rho, 16 * dim * dim);
+	if (part)
+		dev_free(part, pbytes);
 	if (M)
 		dev_free(M, 16ull << n);
-	if (bs != CUBLAS_STATUS_SUCCESS) {
-		snprintf(g.err, sizeof(g.err), "cublasZherk failed (%d)", (int)bs);
-		return DK_ERR_CUDA;
-	}
 	if (e != cudaSuccess)
 		return cuda_fail(e);
 	return DK_OK;

@@ -287,6 +287,35 @@ def test_reduced_density_vs_oracle(dk_gpu, orc, oracle_mod):
     assert abs(d.funmatrix_trace(pt, False) - np.trace(want)) < 1e-11
 
 
+@pytest.mark.parametrize("n,keep_bits,prec", [(12, 3, 2), (16, 5, 2), (16, 6, 2), (18, 8, 2),
+                                               (20, 10, 2), (18, 7, 1), (17, 9, 2)])
+def test_reduced_density_sizes(dk_gpu, orc, oracle_mod, n, keep_bits, prec):
+    """The tensor-core product X X^H over kept sets from 8 to 1024 amplitudes:
+    one or many output tiles, split and unsplit traced ranges, contiguous and
+    scattered kept qubits, complex128 and complex64 registers."""
+    d = dk_gpu
+    rng = W.rng_for(1300 + n + keep_bits)
+    ops = random_ops(rng, n, 60)
+    ops += [W.Op(W.u3(*rng.uniform(0, 2 * np.pi, 3)), [q]) for q in range(n)]
+    a = W.run_ops(d, d.registry_new(n, False, prec), ops)
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    for scattered in (False, True):
+        if scattered:
+            kept = sorted(int(x) for x in rng.choice(n, size=keep_bits, replace=False))
+        else:
+            kept = list(range(keep_bits))
+        keep = sum(1 << q for q in kept)
+        traced = [q for q in range(n) if q not in kept]
+        pt = d.registry_density(a, False)
+        for q in sorted(traced, reverse=True):
+            pt = d.funmatrix_partialtrace(pt, q, False)
+        got = d.funmatrix_numpy(pt)
+        want = oracle_mod.reduced_density(b, keep)
+        tol = ATOL_C128 if prec == 2 else ATOL_C64
+        assert np.allclose(got, want, atol=tol, rtol=0), (scattered, np.abs(got - want).max())
+        assert np.allclose(got, got.conj().T, atol=1e-14)
+
+
 def test_join_vs_oracle(dk_gpu, orc):
     d = dk_gpu
     oa = random_ops(W.rng_for(51), 9, 60)

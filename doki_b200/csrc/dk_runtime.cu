@@ -53,6 +53,7 @@ struct Ctx {
 	int tile_bits = 0; /* 0: planner default */
 	int fold = 0; /* pass-folding cost: 0 planner default, < 0 off */
 	int tensor = 0; /* tensor-core sweeps: 0 planner default (on), < 0 off */
+	int low_bits = -1; /* qubits always in a sweep's tile: < 0 planner default */
 	std::atomic<unsigned long long> sweeps{ 0 }, gates{ 0 }, h2d{ 0 }, d2h{ 0 };
 	char err[256] = { 0 };
 };
@@ -269,6 +270,8 @@ int flush(dk_state *s)
 	lim.tensor = g.tensor;
 	dk_plan_default_limits(prec, n, &lim);
 	lim.fuse = g.fuse;
+	if (g.low_bits >= 0 && g.low_bits <= lim.tile_bits)
+		lim.low_bits = g.low_bits;
 	dk_plan plan;
 	int rc = dk_plan_build(ops.data(), (int)cnt, n, prec, &lim, &plan);
 	if (rc)
@@ -516,6 +519,9 @@ int dk_init(int device)
 	const char *fo = getenv("DK_FOLD");
 	if (fo)
 		g.fold = atoi(fo);
+	const char *lb = getenv("DK_LOW_BITS");
+	if (lb)
+		g.low_bits = atoi(lb);
 	const char *te = getenv("DK_TENSOR");
 	if (te)
 		g.tensor = atoi(te) ? 0 : -1;

@@ -140,6 +140,23 @@ def committed_traffic():
 
 # ------------------------------------------------------------------ engine --
 
+def max_over_ranks(values, world, device):
+    """Element-wise maximum of per-rank timings over all ranks (every rank
+    receives it); replicas are timed by their slowest member."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return t.tolist()
+
+
+def job_rate(world, units_per_rank, seconds):
+    """Whole-job throughput of `world` replicas that each processed
+    `units_per_rank` units in `seconds` (the max over ranks)."""
+    return world * units_per_rank / seconds
+
+
 def run_job(d, c, gates, keep, rolls_mask, rolls):
     """One full workload through the public API; returns the host results."""
     n = c.num_qubits
@@ -236,14 +253,11 @@ def engine_arm(args, rank, world, local_rank):
     io1 = d.engine_stats()
     barrier()
 
-    if world > 1:
-        t = torch.tensor([dev_ms, e2e_s, sweep_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        dev_ms, e2e_s, sweep_ms = t.tolist()
+    dev_ms, e2e_s, sweep_ms = max_over_ranks([dev_ms, e2e_s, sweep_ms], world, "cuda")
 
     layers = depth * args.steps
-    value = world * layers / (dev_ms / 1e3)
-    e2e_value = world * layers / e2e_s
+    value = job_rate(world, layers, dev_ms / 1e3)
+    e2e_value = job_rate(world, layers, e2e_s)
     state_bytes = 16 << n
     avg_sweep_s = (sweep_ms / 1e3) / max(1, nsweeps)
     achieved = 2 * state_bytes / avg_sweep_s / 1e9

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 
 #include <mutex>
 
@@ -780,6 +781,152 @@ __global__ void __launch_bounds__(256)
 	}
 }
 
+/* ---- joint measurement of several qubits -------------------------------
+ * The reference measures the masked qubits one after the other, highest
+ * first (doki.c:1097-1157): p = P(q = 1) of the register collapsed so far,
+ * outcome = p > roll, collapse and renormalise.  Equivalently, with the
+ * joint distribution J over the k measured qubits (one pass over the
+ * state), each p is the conditional S1 / S_prev of the outcomes decided so
+ * far, and one gather applies all k collapses. */
+
+/* index of the j-th amplitude whose measured bits are zero: j's bits
+ * deposited into the unmeasured positions, one run of positions at a time */
+struct DepRuns {
+	uint8_t src[DK_MAX_QUBITS + 1], dst[DK_MAX_QUBITS + 1], len[DK_MAX_QUBITS + 1];
+	int nruns;
+};
+
+__device__ __forceinline__ uint64_t dep_runs(const DepRuns &r, uint64_t j)
+{
+	uint64_t i = 0;
+	for (int k = 0; k < r.nruns; ++k)
+		i |= ((j >> r.src[k]) & ((1ull << r.len[k]) - 1ull)) << r.dst[k];
+	return i;
+}
+
+__device__ __forceinline__ uint64_t deposit_mask(uint64_t v, uint64_t mask)
+{
+	uint64_t out = 0;
+	for (int b = 0; mask; ++b) {
+		const uint64_t low = mask & (~mask + 1ull);
+		if ((v >> b) & 1ull)
+			out |= low;
+		mask &= mask - 1ull;
+	}
+	return out;
+}
+
+/* partials[bin * nchunk + c] = sum of |amp|^2 over chunk c of the bin */
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_joint(const typename CT<R>::T *__restrict__ in, DepRuns runs, uint64_t mask,
+		uint64_t per_bin, uint64_t chunk, uint64_t nchunk, double *partials)
+{
+	__shared__ DepRuns sr;
+	if (threadIdx.x == 0)
+		sr = runs;
+	__syncthreads();
+	const uint64_t bin = blockIdx.y;
+	const uint64_t vb = deposit_mask(bin, mask);
+	for (uint64_t c = blockIdx.x; c < nchunk; c += gridDim.x) {
+		double sum = 0.0, dummy = 0.0;
+		const uint64_t j0 = c * chunk;
+		uint64_t j1 = j0 + chunk;
+		if (j1 > per_bin)
+			j1 = per_bin;
+		for (uint64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x)
+			sum += sqabs(__ldcs(in + (dep_runs(sr, j) | vb)));
+		block_sum2(dummy, sum);
+		if (threadIdx.x == 0)
+			partials[bin * nchunk + c] = sum;
+		__syncthreads();
+	}
+}
+
+/* joint[bin] = sum of its chunks, in order */
+__global__ void __launch_bounds__(256)
+	k_joint_finalize(const double *partials, uint64_t nchunk, double *joint)
+{
+	double sum = 0.0, dummy = 0.0;
+	for (uint64_t c = threadIdx.x; c < nchunk; c += blockDim.x)
+		sum += partials[blockIdx.x * nchunk + c];
+	block_sum2(dummy, sum);
+	if (threadIdx.x == 0)
+		joint[blockIdx.x] = sum;
+}
+
+/* One warp: outcomes of the k measured qubits, highest first, from the
+ * joint distribution; flags[s] = outcome of step s; *vbits = the outcomes
+ * deposited into the measured positions; sc_out->p_sel = probability of the
+ * whole outcome relative to the stored norm. */
+__global__ void k_decide_joint(const double *joint, int k, const double *rolls, int32_t *flags,
+			       uint64_t *vbits, uint64_t mask, const dk_scal *sc_in,
+			       dk_scal *sc_out)
+{
+	const uint32_t lane = threadIdx.x;
+	const uint32_t nb = 1u << k;
+	/* the first probability is relative to the stored norm, as the
+	 * reference's (data registers need not be normalised); the later ones
+	 * are conditional on the outcomes so far */
+	const double n2 = sc_in->norm * sc_in->norm;
+	uint32_t pm = 0, pv = 0;
+	double prev = n2;
+	for (int st = 0; st < k; ++st) {
+		const int bb = k - 1 - st; /* bin bit of the qubit measured now */
+		double s1 = 0.0, s0 = 0.0;
+		for (uint32_t b = lane; b < nb; b += 32)
+			if ((b & pm) == pv) {
+				if ((b >> bb) & 1u)
+					s1 += joint[b];
+				else
+					s0 += joint[b];
+			}
+		for (int o = 16; o > 0; o >>= 1) {
+			s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+			s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+		}
+		const double p = prev > 0.0 ? s1 / prev : 0.0;
+		const int res = p > rolls[st] ? 1 : 0;
+		pm |= 1u << bb;
+		pv |= (uint32_t)res << bb;
+		prev = res ? s1 : s0;
+		if (lane == 0)
+			flags[st] = res;
+	}
+	if (lane == 0) {
+		*vbits = deposit_mask(pv, mask);
+		sc_out->flag = 0;
+		sc_out->p_sel = n2 > 0.0 ? prev / n2 : 0.0;
+		sc_out->zero_norm = 0;
+	}
+}
+
+/* out[j] = in[j deposited into the unmeasured positions | measured bits] */
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_collapse_joint(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
+			 DepRuns runs, uint64_t size, const uint64_t *vbits, double *partials)
+{
+	typedef typename CT<R>::T C2;
+	__shared__ DepRuns sr;
+	if (threadIdx.x == 0)
+		sr = runs;
+	__syncthreads();
+	const uint64_t v = *vbits;
+	double s = 0.0, dummy = 0.0;
+	for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < size;
+	     j += (uint64_t)gridDim.x * blockDim.x) {
+		const C2 x = __ldcs(in + (dep_runs(sr, j) | v));
+		__stcs(out + j, x);
+		s += sqabs(x);
+	}
+	block_sum2(dummy, s);
+	if (threadIdx.x == 0) {
+		partials[2 * blockIdx.x] = 0.0;
+		partials[2 * blockIdx.x + 1] = s;
+	}
+}
+
 /* ---- join (qops.c:97-122) ---------------------------------------------- */
 template <typename R>
 __global__ void __launch_bounds__(256)
@@ -1450,6 +1597,68 @@ cudaError_t launch_measure_collapse(int prec, const void *in, void *out,
 					       FIN_COLLAPSE, 1);
 	}
 	g_launches += (out != nullptr) ? 3 : 1;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_measure_joint(int prec, const void *in, void *out, unsigned n,
+				 uint64_t mask, const double *rolls_dev, int32_t *flags_dev,
+				 const dk_scal *sc_in, dk_scal *sc_out, const Scratch &s,
+				 cudaStream_t st)
+{
+	const int k = __builtin_popcountll(mask);
+	if (k < 1 || k > kJointMaxQubits || (unsigned)k > n)
+		return cudaErrorInvalidValue;
+	DepRuns runs;
+	memset(&runs, 0, sizeof(runs));
+	unsigned src = 0;
+	for (unsigned q = 0; q < n;) {
+		if ((mask >> q) & 1u) {
+			++q;
+			continue;
+		}
+		unsigned e = q;
+		while (e < n && !((mask >> e) & 1u))
+			++e;
+		runs.src[runs.nruns] = (uint8_t)src;
+		runs.dst[runs.nruns] = (uint8_t)q;
+		runs.len[runs.nruns] = (uint8_t)(e - q);
+		runs.nruns++;
+		src += e - q;
+		q = e;
+	}
+	const uint64_t nbins = 1ull << k, per_bin = 1ull << (n - k);
+	/* chunks of >= 4096 amplitudes, at most kJointPartials partials */
+	uint64_t nchunk = (per_bin + 4095) / 4096;
+	if (nchunk * nbins > kJointPartials)
+		nchunk = kJointPartials / nbins;
+	if (nchunk < 1)
+		nchunk = 1;
+	const uint64_t chunk = (per_bin + nchunk - 1) / nchunk;
+	double *part = s.partials;
+	double *joint = s.partials + kJointPartials;
+	uint64_t *vbits = reinterpret_cast<uint64_t *>(s.u64 + 1);
+	uint64_t gx = nchunk < (uint64_t)g_num_sms * 8 ? nchunk : (uint64_t)g_num_sms * 8;
+	dim3 grid((unsigned)gx, (unsigned)nbins);
+	if (prec == DK_C128)
+		k_joint<double><<<grid, 256, 0, st>>>((const double2 *)in, runs, mask, per_bin,
+						      chunk, nchunk, part);
+	else
+		k_joint<float><<<grid, 256, 0, st>>>((const float2 *)in, runs, mask, per_bin, chunk,
+						     nchunk, part);
+	k_joint_finalize<<<(unsigned)nbins, 256, 0, st>>>(part, nchunk, joint);
+	k_decide_joint<<<1, 32, 0, st>>>(joint, k, rolls_dev, flags_dev, vbits, mask, sc_in, sc_out);
+	g_launches += 3;
+	if (out != nullptr) {
+		const int blocks = grid_for(per_bin, 256 * 4, g_num_sms * 8);
+		if (prec == DK_C128)
+			k_collapse_joint<double><<<blocks, 256, 0, st>>>(
+				(const double2 *)in, (double2 *)out, runs, per_bin, vbits, s.partials);
+		else
+			k_collapse_joint<float><<<blocks, 256, 0, st>>>(
+				(const float2 *)in, (float2 *)out, runs, per_bin, vbits, s.partials);
+		k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc_in, sc_out, FIN_COLLAPSE, 1);
+		g_launches += 2;
+	}
 	return cudaGetLastError();
 }
 

@@ -62,6 +62,18 @@ cudaError_t launch_measure_collapse(int prec, const void *in, void *out,
 				    dk_scal *sc_out, const Scratch &s,
 				    cudaStream_t st);
 
+/* Measurement of the k = popcount(mask) <= kJointMaxQubits qubits of mask,
+ * highest first, in one pass: joint distribution, sequential outcomes with
+ * the device rolls rolls_dev[0..k) (flags_dev[s] = outcome of step s),
+ * then, when out is not null, one gather of the 2^(n-k) selected
+ * amplitudes with norm = norm_in * sqrt(P(outcomes)). */
+constexpr int kJointMaxQubits = 12;
+constexpr uint64_t kJointPartials = 131072; /* doubles of s.partials used */
+cudaError_t launch_measure_joint(int prec, const void *in, void *out, unsigned n,
+				 uint64_t mask, const double *rolls_dev, int32_t *flags_dev,
+				 const dk_scal *sc_in, dk_scal *sc_out, const Scratch &s,
+				 cudaStream_t st);
+
 /* out = (most / n1) (x) (least / n2), norm 1 */
 cudaError_t launch_join(int prec, const void *most, unsigned n1,
 			const dk_scal *sc1, const void *least, unsigned n2,

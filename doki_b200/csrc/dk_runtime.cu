@@ -985,6 +985,68 @@ int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 	if (need == 0)
 		return dk_state_clone(s, out);
 
+	if (need <= (unsigned)dk::kJointMaxQubits) {
+		/* one pass: joint distribution of the measured qubits, outcomes
+		 * decided on the device highest qubit first, one gather */
+		double *rolls_dev = CUR.scratch.marg;
+		int32_t *flags_dev = reinterpret_cast<int32_t *>(CUR.scratch.marg + 32);
+		dk_buf *nb = nullptr;
+		dk_scal *sel = nullptr;
+		if (need < n0)
+			rc = buf_new(n0 - need, s->prec, &nb);
+		else
+			rc = dev_alloc((void **)&sel, sizeof(dk_scal));
+		if (rc)
+			return rc;
+		int32_t fl[64];
+		cudaError_t e = cudaMemcpyAsync(rolls_dev, rolls, sizeof(double) * need,
+						cudaMemcpyHostToDevice, CUR.st);
+		g.h2d += sizeof(double) * need;
+		if (e == cudaSuccess)
+			e = dk::launch_measure_joint(s->prec, s->buf->d, nb ? nb->d : nullptr, n0,
+						     mask & full, rolls_dev, flags_dev, s->buf->sc,
+						     nb ? nb->sc : sel, CUR.scratch, CUR.st);
+		if (e == cudaSuccess)
+			e = cudaMemcpyAsync(fl, flags_dev, sizeof(int32_t) * need,
+					    cudaMemcpyDeviceToHost, CUR.st);
+		g.d2h += sizeof(int32_t) * need;
+		dk_scal sc;
+		memset(&sc, 0, sizeof(sc));
+		if (e == cudaSuccess && nb)
+			e = cudaMemcpyAsync(&sc, nb->sc, sizeof(sc), cudaMemcpyDeviceToHost, CUR.st);
+		if (e == cudaSuccess)
+			e = cudaStreamSynchronize(CUR.st);
+		if (sel)
+			dev_free(sel, sizeof(dk_scal));
+		if (e != cudaSuccess) {
+			if (nb)
+				buf_release(nb);
+			return cuda_fail(e);
+		}
+		if (nb && sc.zero_norm) {
+			buf_release(nb);
+			return DK_ERR_NORM0;
+		}
+		unsigned st = 0;
+		for (unsigned i = 0; i < n0; ++i) {
+			const unsigned q = n0 - i - 1;
+			if ((mask >> q) & 1u)
+				results[i] = (int8_t)fl[st++];
+		}
+		if (!nb) {
+			*out = nullptr;
+			return DK_OK;
+		}
+		dk_state *ns = state_alloc(n0 - need, s->prec, s->slot);
+		if (!ns) {
+			buf_release(nb);
+			return DK_ERR_ALLOC;
+		}
+		ns->buf = nb;
+		*out = ns;
+		return DK_OK;
+	}
+
 	rc = marginals_to_scratch(s);
 	if (rc)
 		return rc;

@@ -262,6 +262,52 @@ def test_measure_sequence_vs_oracle(dk_gpu, orc):
             assert np.allclose(allamps(d, ra), orc.registry_get_all(rb), atol=ATOL_C128, rtol=0)
 
 
+@pytest.mark.parametrize("n,prec", [(22, 2), (20, 1), (13, 2)])
+def test_measure_joint_vs_oracle(dk_gpu, orc, n, prec):
+    """Measurement of 1 to 12 qubits in one pass (joint distribution of the
+    measured qubits, outcomes decided highest first, one collapse): the
+    outcomes equal the reference sequence's and the collapsed register the
+    oracle's, for masks with low, high and scattered qubits."""
+    d = dk_gpu
+    rng = W.rng_for(600 + n)
+    ops = random_ops(rng, n, 80)
+    ops += [W.Op(W.u3(*rng.uniform(0, 2 * np.pi, 3)), [q]) for q in range(n)]
+    a = W.run_ops(d, d.registry_new(n, False, prec), ops)
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    masks = [1, 1 << (n - 1), 0b1011, (1 << (n - 1)) | 1 | (1 << (n // 2)),
+             sum(1 << int(q) for q in rng.choice(n, size=min(12, n), replace=False)),
+             sum(1 << int(q) for q in rng.choice(n, size=5, replace=False))]
+    for mask in masks:
+        for _ in range(3):
+            rolls = rng.random(bin(mask).count("1")).tolist()
+            ra, resa = d.registry_measure(a, mask, rolls, 1, False)
+            rb, resb = orc.registry_measure(b, mask, rolls)
+            assert res_list(resa) == res_list(resb), (mask, rolls)
+            if rb is not None:
+                tol = ATOL_C128 if prec == 2 else ATOL_C64
+                assert np.allclose(allamps(d, ra), orc.registry_get_all(rb), atol=tol, rtol=0)
+
+
+def test_measure_joint_unnormalised_data(dk_gpu, orc):
+    """Data registers are not normalised: the first outcome compares the
+    probability relative to the stored norm, as the reference does."""
+    d = dk_gpu
+    rng = W.rng_for(77)
+    n = 9
+    vals = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)) * 0.07
+    a = d.registry_new_data(n, vals.tolist(), False)
+    b = orc.registry_new_data(n, vals.tolist())
+    for mask in (0b101, 0b110000001, (1 << n) - 1):
+        for _ in range(4):
+            rolls = rng.random(bin(mask).count("1")).tolist()
+            ra, resa = d.registry_measure(a, mask, rolls, 1, False)
+            rb, resb = orc.registry_measure(b, mask, rolls)
+            assert res_list(resa) == res_list(resb), (mask, rolls)
+            if rb is not None:
+                assert np.allclose(allamps(d, ra), orc.registry_get_all(rb), atol=ATOL_C128,
+                                   rtol=0)
+
+
 def test_reduced_density_vs_oracle(dk_gpu, orc, oracle_mod):
     d = dk_gpu
     n = 14

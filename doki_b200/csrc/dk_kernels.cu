@@ -690,13 +690,42 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
 	for (int j = 0; j < kMargHi; ++j)
 		hi[j] = 0.0;
-	for (uint64_t k = 0; k < cnt; ++k) {
-		const double p = sqabs(__ldcs(d + ((k << s) | g)));
-		tot += p;
+	if (cnt >= 16) {
+		/* 16 consecutive k at a time: the 4 low bits of k take fixed
+		 * patterns, every higher bit is constant over the group */
+		for (uint64_t k0 = 0; k0 < cnt; k0 += 16) {
+			double p[16];
 #pragma unroll
-		for (int j = 0; j < kMargHi; ++j)
-			if (j < nb && ((k >> j) & 1u))
-				hi[j] += p;
+			for (int e = 0; e < 16; ++e)
+				p[e] = sqabs(__ldcs(d + (((k0 + e) << s) | g)));
+			double t = 0.0;
+#pragma unroll
+			for (int e = 0; e < 16; ++e)
+				t += p[e];
+#pragma unroll
+			for (int j = 0; j < 4; ++j) {
+				double h = 0.0;
+#pragma unroll
+				for (int e = 0; e < 16; ++e)
+					if ((e >> j) & 1)
+						h += p[e];
+				hi[j] += h;
+			}
+#pragma unroll
+			for (int j = 4; j < kMargHi; ++j)
+				if (j < nb && ((k0 >> j) & 1u))
+					hi[j] += t;
+			tot += t;
+		}
+	} else {
+		for (uint64_t k = 0; k < cnt; ++k) {
+			const double p = sqabs(__ldcs(d + ((k << s) | g)));
+			tot += p;
+#pragma unroll
+			for (int j = 0; j < kMargHi; ++j)
+				if (j < nb && ((k >> j) & 1u))
+					hi[j] += p;
+		}
 	}
 	__shared__ double red[32];
 	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;

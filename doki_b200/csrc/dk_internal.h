@@ -156,6 +156,11 @@ enum {
 	DK_PASS_CTL = 1u, /* a gate of the pass has controls inside the tile */
 	DK_PASS_WARP = 2u, /* the next pass maps the same tile bits to the warp
 			    * index: a warp barrier separates the two */
+	DK_PASS_CHAIN = 4u, /* tensor sweeps: this pass and the next each hold one
+			     * entry, and this pass's thread bits 0-2 are the next
+			     * pass's bits in the order that makes this pass's MMA
+			     * output the next pass's MMA input: the pair runs in
+			     * registers between one gather and one scatter */
 };
 
 typedef struct dk_sweep_hdr {

@@ -294,6 +294,40 @@ __device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], con
  * and writes amplitude l/4 of columns 2(l%4) and 2(l%4)+1.  Entries with
  * controls off the pass bits write only the columns whose tile index
  * satisfies them; the others keep their values in the shared tile. */
+/* Matrix of a gate-list entry of a tensor sweep (whole 8x8 matrices), the
+ * tile's variant picked by its conditions. */
+__device__ __forceinline__ uint32_t tc_matrix(const uint4 &d, const dk_gate_cond *scond,
+					      uint64_t base)
+{
+	uint32_t mi = d.x >> 16;
+	if ((d.x & 0xffffu) == DK_GC_DENSE3V)
+		for (uint32_t c = 0; c < d.w; ++c) {
+			const dk_gate_cond cc = scond[(d.z >> (10 * c)) & 1023u];
+			if (((base & cc.gc) == cc.gc) && !(base & cc.ga))
+				mi += 1u << c;
+		}
+	return mi;
+}
+
+/* y = M x for one column group, Gauss form: Mr xr, Mi xi, (Mr + Mi)(xr + xi)
+ * as three real 8x8 products of two k-steps each; y = (yr[2t], yr[2t+1],
+ * yi[2t], yi[2t+1]) of output amplitude l/4. */
+__device__ __forceinline__ void tc_product(const double2 &e0, const double2 &e1, const double2 &x0,
+					   const double2 &x1, double (&y)[4])
+{
+	double p1[2] = { 0.0, 0.0 }, p2[2] = { 0.0, 0.0 }, p3[2] = { 0.0, 0.0 };
+	dmma(p1[0], p1[1], e0.x, x0.x);
+	dmma(p2[0], p2[1], e0.y, x0.y);
+	dmma(p3[0], p3[1], e0.x + e0.y, x0.x + x0.y);
+	dmma(p1[0], p1[1], e1.x, x1.x);
+	dmma(p2[0], p2[1], e1.y, x1.y);
+	dmma(p3[0], p3[1], e1.x + e1.y, x1.x + x1.y);
+	y[0] = p1[0] - p2[0];
+	y[1] = p1[1] - p2[1];
+	y[2] = p3[0] - p1[0] - p2[0];
+	y[3] = p3[1] - p1[1] - p2[1];
+}
+
 template <typename R, int SW, int M, int MINB, int NBUF>
 __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 	k_sweep_tc(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
@@ -429,6 +463,56 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		}
 		for (int p = 0; p < npass; ++p) {
 			const dk_pass_desc *pd = passes + p;
+			if (__ldg(&pd->flags) & DK_PASS_CHAIN) {
+				/* this pass and the next, one entry each: this pass's
+				 * MMA output is the next pass's MMA input in place */
+				const dk_pass_desc *pn = pd + 1;
+				const uint32_t shw = __ldg(&pd->shi[warp]);
+				const uint32_t t8 = __ldg(&pd->slo[8]), t16 = __ldg(&pd->slo[16]);
+				const uint32_t sgl = __ldg(&pd->slo[gl]) ^ shw;
+				const uint32_t s0 = __ldg(&pd->sp[0]), s1 = __ldg(&pd->sp[1]),
+					       s2 = __ldg(&pd->sp[2]);
+				const uint32_t gj0 = ((gk & 1u) ? s0 : 0u) ^ ((gk & 2u) ? s1 : 0u);
+				const uint32_t gj1 = gj0 ^ s2;
+				const uint32_t shn = __ldg(&pn->shi[warp]);
+				const uint32_t u8 = __ldg(&pn->slo[8]), u16 = __ldg(&pn->slo[16]);
+				const uint32_t sgk = __ldg(&pn->slo[2u * gk]) ^ shn, u1 = __ldg(&pn->slo[1]);
+				const uint32_t n0 = __ldg(&pn->sp[0]), n1 = __ldg(&pn->sp[1]),
+					       n2 = __ldg(&pn->sp[2]);
+				const uint32_t sr = ((gl & 1u) ? n0 : 0u) ^ ((gl & 2u) ? n1 : 0u) ^
+						    ((gl & 4u) ? n2 : 0u);
+				/* lane fragments: entries (l/4, l%4) and (l/4, 4 + l%4) */
+				const double2 *ma = mats + 64 * (size_t)tc_matrix(sg[__ldg(&pd->g0)],
+										  scond, base) +
+						    8 * gl + gk;
+				const double2 *mb = mats + 64 * (size_t)tc_matrix(sg[__ldg(&pn->g0)],
+										  scond, base) +
+						    8 * gl + gk;
+				const double2 e0 = __ldg(ma), e1 = __ldg(ma + 4);
+#pragma unroll
+				for (int q = 0; q < 4; ++q) {
+					const uint32_t bg = sgl ^ ((q & 1) ? t8 : 0u) ^ ((q & 2) ? t16 : 0u);
+					const double2 x0 = to_c128(tile[bg ^ gj0]);
+					const double2 x1 = to_c128(tile[bg ^ gj1]);
+					double y[4], z[4];
+					tc_product(e0, e1, x0, x1, y);
+					/* amplitude l%4 and 4 + l%4 of column l/4 in the next pass */
+					tc_product(__ldg(mb), __ldg(mb + 4), make_double2(y[0], y[2]),
+						   make_double2(y[1], y[3]), z);
+					__syncwarp(); /* the group's gathers precede its writes */
+#pragma unroll
+					for (int e = 0; e < 2; ++e) {
+						const uint32_t bs = sgk ^ (e ? u1 : 0u) ^ ((q & 1) ? u8 : 0u) ^
+								    ((q & 2) ? u16 : 0u);
+						tile[bs ^ sr] = from_c128<C2>(make_double2(z[e], z[2 + e]));
+					}
+				}
+				__syncwarp();
+				++p;
+				if (!(__ldg(&pn->flags) & DK_PASS_WARP))
+					__syncthreads();
+				continue;
+			}
 			/* the slot tables are XOR-linear in the thread index: a column's
 			 * slot is the XOR of the entries of its set bits */
 			const uint32_t shw = __ldg(&pd->shi[warp]);

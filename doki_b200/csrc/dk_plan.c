@@ -286,6 +286,115 @@ static int tc_best(uint32_t P, uint32_t L, int m, int res, uint8_t *pb, uint8_t 
 	return best;
 }
 
+/* What build_phase needs to know about the gates of a sweep (tensor
+ * sweeps) to decide which pairs of passes can chain in registers. */
+typedef struct phase_ctx {
+	const dk_flat_op *ops;
+	const int *order; /* gates of the sweep in pass order */
+	const int8_t *loc_of; /* tile bit of each qubit, -1 outside the tile */
+	unsigned n;
+} phase_ctx;
+
+static int tc_local(const dk_flat_op *op, const int8_t *loc_of, const uint32_t *preg);
+static void tile_cond(const dk_flat_op *op, const int8_t *loc_of, unsigned n, uint64_t *gc,
+		      uint64_t *ga);
+
+/* A pass of a tensor sweep folds into exactly one gate-list entry when all
+ * its gates are pass-local and carry at most DK_VAR_MAX distinct tile
+ * conditions. */
+static int single_entry(const phase_ctx *cx, const dk_pass_desc *pd, uint32_t P)
+{
+	if (pd->g1 <= pd->g0)
+		return 0;
+	uint32_t preg[64];
+	memset(preg, 0xff, sizeof(preg));
+	int r = 0;
+	for (int b = 0; b < 32; b++)
+		if (P >> b & 1u)
+			preg[b] = (uint32_t)r++;
+	uint64_t cgc[DK_VAR_MAX], cga[DK_VAR_MAX];
+	int nv = 0;
+	for (int g = pd->g0; g < pd->g1; g++) {
+		const dk_flat_op *op = &cx->ops[cx->order[g]];
+		if (!tc_local(op, cx->loc_of, preg))
+			return 0;
+		uint64_t gc, ga;
+		tile_cond(op, cx->loc_of, cx->n, &gc, &ga);
+		if (!(gc | ga))
+			continue;
+		int j = 0;
+		while (j < nv && (cgc[j] != gc || cga[j] != ga))
+			j++;
+		if (j == nv) {
+			if (nv == DK_VAR_MAX)
+				return 0;
+			cgc[nv] = gc;
+			cga[nv] = ga;
+			nv++;
+		}
+	}
+	return 1;
+}
+
+/* Lane tables of a chained pair: pass A (bits a0 a1 a2, thread bits c0 c1
+ * c2 r0 r1 W...) and pass B = (c1 c2 c0, thread bits a0 a1 a2 r0 r1 W...),
+ * the orders picked for the fewest shared-memory wavefronts of A's gather
+ * and B's scatter. */
+static void chain_pair(dk_pass_desc *pa, dk_pass_desc *pb, uint32_t PA, uint32_t PB, uint32_t W,
+		       int m, int res, uint8_t *pbA, uint8_t *pbB)
+{
+	int a[3], c[3], r[2], na = 0, nc = 0, nr = 0;
+	for (int b = 0; b < m; b++) {
+		if (PA >> b & 1u)
+			a[na++] = b;
+		else if (PB >> b & 1u)
+			c[nc++] = b;
+		else if (!(W >> b & 1u) && nr < 2)
+			r[nr++] = b;
+	}
+	static const int perm[6][3] = { { 0, 1, 2 }, { 0, 2, 1 }, { 1, 0, 2 },
+					{ 1, 2, 0 }, { 2, 0, 1 }, { 2, 1, 0 } };
+	int best = 1 << 30, bo = 0, bp = 0;
+	for (int o = 0; o < 6; o++)
+		for (int q = 0; q < 6; q++) {
+			const int a0 = a[perm[o][0]], a1 = a[perm[o][1]], a2 = a[perm[o][2]];
+			const int c0 = c[perm[q][0]], c1 = c[perm[q][1]], c2 = c[perm[q][2]];
+			int cost;
+			if (res == 3) {
+				const int g[3] = { c0, a0, a1 }, t[3] = { c1, a1, a2 };
+				cost = (1 << (3 - nres(g, 3, 3))) + (1 << (3 - nres(t, 3, 3)));
+			} else {
+				const int g[4] = { c0, c1, a0, a1 }, t[4] = { c1, c2, a1, a2 };
+				cost = (1 << (4 - nres(g, 4, res))) + (1 << (4 - nres(t, 4, res)));
+			}
+			if (cost < best) {
+				best = cost;
+				bo = o;
+				bp = q;
+			}
+		}
+	uint8_t laneA[32], laneB[32];
+	int nl = 0;
+	for (int j = 0; j < 3; j++) {
+		pbA[j] = (uint8_t)a[perm[bo][j]];
+		laneA[j] = (uint8_t)c[perm[bp][j]];
+		laneB[j] = pbA[j];
+	}
+	pbB[0] = laneA[1];
+	pbB[1] = laneA[2];
+	pbB[2] = laneA[0];
+	nl = 3;
+	for (int j = 0; j < nr; j++, nl++)
+		laneA[nl] = laneB[nl] = (uint8_t)r[j];
+	for (int b = 0; b < m; b++)
+		if (W >> b & 1u) {
+			laneA[nl] = laneB[nl] = (uint8_t)b;
+			nl++;
+		}
+	pass_tables_lanes(pa, pbA, laneA, nl, res);
+	pass_tables_lanes(pb, pbB, laneB, nl, res);
+}
+
 /* A phase: consecutive passes [0, cnt) whose pass bits all avoid the same
  * `wbits` tile bits W, which every pass maps to the thread bits above the 5
  * lane bits.  A warp then touches the same tile slots in every pass of the
@@ -293,7 +402,8 @@ static int tc_best(uint32_t P, uint32_t L, int m, int res, uint8_t *pb, uint8_t 
  * target bits of pass i; they are filled up to DK_PASS_BITS from the phase's
  * union first (keeping it small), W is picked from the rest. */
 static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, int wbits,
-			int res, int tensor, uint8_t (*pbits)[DK_PASS_BITS])
+			int res, int tensor, const phase_ctx *cx,
+			uint8_t (*pbits)[DK_PASS_BITS])
 {
 	uint32_t F = 0, pmask[64];
 	for (int i = 0; i < cnt; i++)
@@ -339,6 +449,18 @@ static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, 
 	}
 	if (tensor) {
 		for (int i = 0; i < cnt; i++) {
+			/* a pair of single-entry passes on disjoint bits chains */
+			if (cx && wbits >= 0 && i + 1 < cnt && !(pmask[i] & pmask[i + 1]) &&
+			    single_entry(cx, &pd[i], pmask[i]) &&
+			    single_entry(cx, &pd[i + 1], pmask[i + 1])) {
+				chain_pair(&pd[i], &pd[i + 1], pmask[i], pmask[i + 1], W, m, res,
+					   pbits[i], pbits[i + 1]);
+				pd[i].flags |= DK_PASS_WARP | DK_PASS_CHAIN;
+				if (i + 2 < cnt)
+					pd[i + 1].flags |= DK_PASS_WARP;
+				i++;
+				continue;
+			}
 			uint8_t lane[32], l3[3];
 			const uint32_t L = ((1u << m) - 1u) & ~pmask[i] & ~W;
 			tc_best(pmask[i], L, m, res, pbits[i], l3);
@@ -653,6 +775,7 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	 * target bits fit in m - wbits tile bits (wbits = thread bits above the
 	 * lanes).  Narrower tiles fill each pass with the highest free bits. */
 	const int wbits = m - DK_PASS_BITS - 5;
+	const phase_ctx cx = { ops, order, loc_of, n };
 	for (int p0 = 0; p0 < npass;) {
 		int p1 = p0 + 1;
 		if (wbits >= 0) {
@@ -660,7 +783,7 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 			while (p1 < npass && p1 - p0 < 64 && popc(U | need[p1]) <= m - wbits)
 				U |= need[p1++];
 			build_phase(&passes[p0], &need[p0], p1 - p0, m, wbits, res, fold->tensor,
-				    &pbits[p0]);
+				    fold->tensor ? &cx : NULL, &pbits[p0]);
 		} else {
 			uint32_t P = need[p0];
 			for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
@@ -730,8 +853,11 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 					e++;
 				}
 				/* one condition shared by every gate of the run: a plain
-				 * entry skipped by the other tiles */
-				if (it->nvar == 1 && all_cond) {
+				 * entry skipped by the other tiles (chained passes keep
+				 * the identity as the other variant instead) */
+				const int chained = (passes[pi].flags & DK_PASS_CHAIN) ||
+						    (pi > 0 && (passes[pi - 1].flags & DK_PASS_CHAIN));
+				if (it->nvar == 1 && all_cond && !chained) {
 					it->nvar = 0;
 					it->has_cond = 1;
 				}
@@ -813,6 +939,10 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 			g++;
 		}
 		passes[pi].g1 = (uint16_t)nit;
+		/* a chained pair needs exactly one entry in each pass */
+		if (pi > 0 && (passes[pi - 1].flags & DK_PASS_CHAIN) &&
+		    (passes[pi - 1].g1 - passes[pi - 1].g0 != 1 || passes[pi].g1 - passes[pi].g0 != 1))
+			passes[pi - 1].flags &= ~(uint32_t)DK_PASS_CHAIN;
 		/* controls inside the tile, after folding */
 		passes[pi].flags &= ~(uint32_t)DK_PASS_CTL;
 		for (int k = passes[pi].g0; k < nit; k++) {

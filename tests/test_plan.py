@@ -420,3 +420,45 @@ def test_tensor_variants_fold_out_of_tile_conditions(lib, orc):
         g = np.frombuffer(blob, GATE, int(h["ngate"]), off + int(h["gate_off"]))
         nvar += int((g["code"] == 45).sum())
     assert nvar > 0
+
+
+def thread_bits(p, m):
+    """Tile bit carried by each thread-index bit of a pass (from rlo / rhi)."""
+    out = []
+    for j in range(m - 3):
+        raw = int(p["rlo"][1 << j]) if j < 5 else int(p["rhi"][1 << (j - 5)])
+        out.append(raw.bit_length() - 1)
+    return out
+
+
+def pass_bits(p):
+    return [int(p["pm"][j]).bit_length() - 1 for j in range(3)]
+
+
+@pytest.mark.parametrize("prec,n", [(2, 30), (1, 30), (2, 16)])
+def test_chained_pairs_keep_the_mma_layout(lib, prec, n):
+    """A pass flagged DK_PASS_CHAIN and the next one each hold one entry, the
+    first pass's thread bits 0-2 (c0 c1 c2) are the second pass's bits in the
+    order (c1 c2 c0), the second pass's thread bits 0-2 are the first pass's
+    bits in order, and both keep the remaining thread bits: the MMA output
+    layout of the first is the input layout of the second."""
+    c = W.scale_circuit(seed=2, n=n, depth=12)
+    steps, blob = build_plan(lib, c.ops, n, prec=prec)
+    chained = total = 0
+    for kind, off, _ in steps:
+        h = np.frombuffer(blob, HDR, 1, off)[0]
+        m = int(h["m"])
+        passes = np.frombuffer(blob, PASS, int(h["npass"]), off + int(h["pass_off"]))
+        total += len(passes)
+        for i, p in enumerate(passes):
+            if not int(p["flags"]) & 4:
+                continue
+            chained += 1
+            q = passes[i + 1]
+            assert int(p["g1"]) - int(p["g0"]) == 1 and int(q["g1"]) - int(q["g0"]) == 1
+            assert int(p["flags"]) & 2  # same warp bits
+            ta, tb = thread_bits(p, m), thread_bits(q, m)
+            assert pass_bits(q) == [ta[1], ta[2], ta[0]]
+            assert tb[:3] == pass_bits(p)
+            assert ta[3:] == tb[3:]
+    assert chained > 0 and chained * 2 <= total

@@ -82,6 +82,7 @@ struct dk_state {
 
 #define DK_TILE_BITS_C128 11
 #define DK_TILE_BITS_C64 11
+#define DK_TILE_BITS_TC 12 /* tile bits of tensor-core sweeps */
 #define DK_PASS_BITS 3
 /* nibbles of a tile number (tile bits m >= 0, register <= 40 qubits) */
 #define DK_DEP_NIBBLES 10

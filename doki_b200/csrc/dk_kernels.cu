@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 #define DK_TC_MINB11 3
 #endif
 #ifndef DK_TC_MINB12
-#define DK_TC_MINB12 1
+#define DK_TC_MINB12 3
 #endif
 
 
@@ -329,7 +329,7 @@ __device__ __forceinline__ void tc_product(const double2 &e0, const double2 &e1,
 }
 
 template <typename R, int SW, int M, int MINB, int NBUF>
-__global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
+__global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 	k_sweep_tc(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
 		   const unsigned char *__restrict__ prog, double *partials)
 {
@@ -339,6 +339,8 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 	const int m = h->m;
 	const int lanes = m - PB;
 	const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+	/* 12-bit tiles: 256 threads, thread t owns columns t and t + 256 */
+	constexpr int VT = (M >= 12) ? 2 : 1;
 	const int npass = h->npass, ngate = h->ngate;
 	const uint32_t tn_amp = 1u << m;
 	const int ncond = (int)h->ncond;
@@ -382,11 +384,18 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		}
 		sdep[e >> 4][e & 15] = v;
 	}
-	uint64_t off_t = 0;
-	for (int j = 0; j < lanes; ++j)
-		if ((tid >> j) & 1u)
-			off_t |= 1ull << sq[j];
-	const uint32_t stid = swz<SW>(tid);
+	uint64_t off_t[VT];
+	uint32_t stid[VT];
+#pragma unroll
+	for (int h = 0; h < VT; ++h) {
+		const uint32_t vt = tid + 256u * h;
+		uint64_t o = 0;
+		for (int j = 0; j < lanes; ++j)
+			if ((vt >> j) & 1u)
+				o |= 1ull << sq[j];
+		off_t[h] = o;
+		stid[h] = swz<SW>(vt);
+	}
 	__syncthreads();
 	const uint64_t ntiles = h->ntiles;
 	const int ndep = (h->n - m + 3) >> 2;
@@ -417,14 +426,17 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		return ntiles;
 	};
 	auto prefetch = [&](uint64_t base, C2 *buf) {
-		const uint64_t bo = base | off_t;
 #pragma unroll
-		for (int r = 0; r < NA; ++r) {
-			C2 *dst = buf + (stid ^ sro[r]);
-			if (sizeof(C2) == 16)
-				cp_async16(dst, in + (bo | soff[r]));
-			else
-				cp_async8(dst, in + (bo | soff[r]));
+		for (int h = 0; h < VT; ++h) {
+			const uint64_t bo = base | off_t[h];
+#pragma unroll
+			for (int r = 0; r < NA; ++r) {
+				C2 *dst = buf + (stid[h] ^ sro[r]);
+				if (sizeof(C2) == 16)
+					cp_async16(dst, in + (bo | soff[r]));
+				else
+					cp_async8(dst, in + (bo | soff[r]));
+			}
 		}
 		cp_async_commit();
 	};
@@ -457,8 +469,10 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 			 * The read uses the identity mapping, so every thread must be
 			 * done with it before the first pass writes the tile. */
 #pragma unroll
-			for (int r = 0; r < NA; ++r)
-				insq += sqabs(tile[stid ^ sro[r]]);
+			for (int h = 0; h < VT; ++h)
+#pragma unroll
+				for (int r = 0; r < NA; ++r)
+					insq += sqabs(tile[stid[h] ^ sro[r]]);
 			__syncthreads();
 		}
 		for (int p = 0; p < npass; ++p) {
@@ -467,16 +481,14 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 				/* this pass and the next, one entry each: this pass's
 				 * MMA output is the next pass's MMA input in place */
 				const dk_pass_desc *pn = pd + 1;
-				const uint32_t shw = __ldg(&pd->shi[warp]);
 				const uint32_t t8 = __ldg(&pd->slo[8]), t16 = __ldg(&pd->slo[16]);
-				const uint32_t sgl = __ldg(&pd->slo[gl]) ^ shw;
+				const uint32_t sgl0 = __ldg(&pd->slo[gl]);
 				const uint32_t s0 = __ldg(&pd->sp[0]), s1 = __ldg(&pd->sp[1]),
 					       s2 = __ldg(&pd->sp[2]);
 				const uint32_t gj0 = ((gk & 1u) ? s0 : 0u) ^ ((gk & 2u) ? s1 : 0u);
 				const uint32_t gj1 = gj0 ^ s2;
-				const uint32_t shn = __ldg(&pn->shi[warp]);
 				const uint32_t u8 = __ldg(&pn->slo[8]), u16 = __ldg(&pn->slo[16]);
-				const uint32_t sgk = __ldg(&pn->slo[2u * gk]) ^ shn, u1 = __ldg(&pn->slo[1]);
+				const uint32_t sgk0 = __ldg(&pn->slo[2u * gk]), u1 = __ldg(&pn->slo[1]);
 				const uint32_t n0 = __ldg(&pn->sp[0]), n1 = __ldg(&pn->sp[1]),
 					       n2 = __ldg(&pn->sp[2]);
 				const uint32_t sr = ((gl & 1u) ? n0 : 0u) ^ ((gl & 2u) ? n1 : 0u) ^
@@ -490,7 +502,10 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 						    8 * gl + gk;
 				const double2 e0 = __ldg(ma), e1 = __ldg(ma + 4);
 #pragma unroll
-				for (int q = 0; q < 4; ++q) {
+				for (int hq = 0; hq < 4 * VT; ++hq) {
+					const int q = hq & 3, h = hq >> 2;
+					const uint32_t sgl = sgl0 ^ __ldg(&pd->shi[warp + 8u * h]);
+					const uint32_t sgk = sgk0 ^ __ldg(&pn->shi[warp + 8u * h]);
 					const uint32_t bg = sgl ^ ((q & 1) ? t8 : 0u) ^ ((q & 2) ? t16 : 0u);
 					const double2 x0 = to_c128(tile[bg ^ gj0]);
 					const double2 x1 = to_c128(tile[bg ^ gj1]);
@@ -515,10 +530,9 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 			}
 			/* the slot tables are XOR-linear in the thread index: a column's
 			 * slot is the XOR of the entries of its set bits */
-			const uint32_t shw = __ldg(&pd->shi[warp]);
 			const uint32_t t8 = __ldg(&pd->slo[8]), t16 = __ldg(&pd->slo[16]);
-			const uint32_t sgl = __ldg(&pd->slo[gl]) ^ shw;
-			const uint32_t sgk = __ldg(&pd->slo[2u * gk]) ^ shw, t1 = __ldg(&pd->slo[1]);
+			const uint32_t sgl0 = __ldg(&pd->slo[gl]);
+			const uint32_t sgk0 = __ldg(&pd->slo[2u * gk]), t1 = __ldg(&pd->slo[1]);
 			const uint32_t s0 = __ldg(&pd->sp[0]), s1 = __ldg(&pd->sp[1]),
 				       s2 = __ldg(&pd->sp[2]);
 			const uint32_t gj0 = ((gk & 1u) ? s0 : 0u) ^ ((gk & 2u) ? s1 : 0u);
@@ -554,7 +568,10 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 				/* one column group at a time: the groups' slots are
 				 * disjoint */
 #pragma unroll
-				for (int q = 0; q < 4; ++q) {
+				for (int hq = 0; hq < 4 * VT; ++hq) {
+					const int q = hq & 3, h = hq >> 2;
+					const uint32_t shw = __ldg(&pd->shi[warp + 8u * h]);
+					const uint32_t sgl = sgl0 ^ shw, sgk = sgk0 ^ shw;
 					const uint32_t bg = sgl ^ ((q & 1) ? t8 : 0u) ^ ((q & 2) ? t16 : 0u);
 					const double2 x0 = to_c128(tile[bg ^ gj0]);
 					const double2 x1 = to_c128(tile[bg ^ gj1]);
@@ -582,7 +599,7 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 						if (ctl) { /* rare: controls off the pass bits */
 							const uint32_t col = (q << 3) | (2u * gk + e);
 							const uint32_t raw = __ldg(&pd->rlo[col]) |
-									     __ldg(&pd->rhi[warp]);
+									     __ldg(&pd->rhi[warp + 8u * h]);
 							if (!ctl_ok(raw, d.z, d.w))
 								continue;
 						}
@@ -596,21 +613,41 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 			if (!(pflags & DK_PASS_WARP))
 				__syncthreads();
 		}
-		C2 a[NA];
+		if (VT == 1) {
+			C2 a[NA];
 #pragma unroll
-		for (int r = 0; r < NA; ++r)
-			a[r] = tile[stid ^ sro[r]];
-		__syncthreads(); /* the buffer is free */
-		if (NBUF == 1) {
-			tn = next_tile(t + gridDim.x);
-			if (tn < ntiles)
-				prefetch(tile_base(tn), bufs);
-		}
-		const uint64_t bo = base | off_t;
+			for (int r = 0; r < NA; ++r)
+				a[r] = tile[stid[0] ^ sro[r]];
+			__syncthreads(); /* the buffer is free */
+			if (NBUF == 1) {
+				tn = next_tile(t + gridDim.x);
+				if (tn < ntiles)
+					prefetch(tile_base(tn), bufs);
+			}
+			const uint64_t bo = base | off_t[0];
 #pragma unroll
-		for (int r = 0; r < NA; ++r) {
-			outsq += sqabs(a[r]);
-			__stcs(out + (bo | soff[r]), a[r]);
+			for (int r = 0; r < NA; ++r) {
+				outsq += sqabs(a[r]);
+				__stcs(out + (bo | soff[r]), a[r]);
+			}
+		} else {
+			/* two column sets: stream each amplitude out as it is read */
+#pragma unroll
+			for (int h = 0; h < VT; ++h) {
+				const uint64_t bo = base | off_t[h];
+#pragma unroll
+				for (int r = 0; r < NA; ++r) {
+					const C2 v = tile[stid[h] ^ sro[r]];
+					outsq += sqabs(v);
+					__stcs(out + (bo | soff[r]), v);
+				}
+			}
+			__syncthreads(); /* the buffer is free */
+			if (NBUF == 1) {
+				tn = next_tile(t + gridDim.x);
+				if (tn < ntiles)
+					prefetch(tile_base(tn), bufs);
+			}
 		}
 		t = tn;
 		cur ^= 1;
@@ -1513,7 +1550,7 @@ static cudaError_t run_sweep_tc(const void *in, void *out, const unsigned char *
 	const uint64_t cap = (uint64_t)num_sms * MINB;
 	if (blocks > cap)
 		blocks = cap;
-	kern<<<(int)blocks, 1 << (m - DK_PASS_BITS), smem, st>>>((const C2 *)in, (C2 *)out,
+	kern<<<(int)blocks, m >= 12 ? 256 : 1 << (m - DK_PASS_BITS), smem, st>>>((const C2 *)in, (C2 *)out,
 								   dprog, s.partials);
 	*blocks_out = (int)blocks;
 	return cudaGetLastError();

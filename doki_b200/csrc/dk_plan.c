@@ -31,6 +31,8 @@ static int popc(uint64_t x) { return __builtin_popcountll(x); }
 void dk_plan_default_limits(int prec, unsigned n, dk_plan_limits *lim)
 {
 	int m = (prec == DK_C64) ? DK_TILE_BITS_C64 : DK_TILE_BITS_C128;
+	if (lim->tensor >= 0)
+		m = DK_TILE_BITS_TC; /* tensor sweeps: 4 passes, two chained pairs */
 	if (lim->tile_bits >= DK_PASS_BITS && lim->tile_bits <= 12)
 		m = lim->tile_bits; /* caller's choice */
 	if ((int)n < m)

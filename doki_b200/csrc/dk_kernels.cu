@@ -384,18 +384,15 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 		}
 		sdep[e >> 4][e & 15] = v;
 	}
-	uint64_t off_t[VT];
-	uint32_t stid[VT];
-#pragma unroll
-	for (int h = 0; h < VT; ++h) {
-		const uint32_t vt = tid + 256u * h;
-		uint64_t o = 0;
-		for (int j = 0; j < lanes; ++j)
-			if ((vt >> j) & 1u)
-				o |= 1ull << sq[j];
-		off_t[h] = o;
-		stid[h] = swz<SW>(vt);
-	}
+	/* column set h of this thread: thread index tid + 256 h; the second set
+	 * differs in thread bit 8 only, so its offsets follow from the first */
+	uint64_t off_t0 = 0;
+	for (int j = 0; j < lanes; ++j)
+		if ((tid >> j) & 1u)
+			off_t0 |= 1ull << sq[j];
+	const uint32_t stid0 = swz<SW>(tid);
+	auto off_t = [&](int h) -> uint64_t { return h ? (off_t0 | (1ull << sq[8])) : off_t0; };
+	auto stid = [&](int h) -> uint32_t { return h ? (stid0 ^ swz<SW>(256u)) : stid0; };
 	__syncthreads();
 	const uint64_t ntiles = h->ntiles;
 	const int ndep = (h->n - m + 3) >> 2;
@@ -428,10 +425,10 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 	auto prefetch = [&](uint64_t base, C2 *buf) {
 #pragma unroll
 		for (int h = 0; h < VT; ++h) {
-			const uint64_t bo = base | off_t[h];
+			const uint64_t bo = base | off_t(h);
 #pragma unroll
 			for (int r = 0; r < NA; ++r) {
-				C2 *dst = buf + (stid[h] ^ sro[r]);
+				C2 *dst = buf + (stid(h) ^ sro[r]);
 				if (sizeof(C2) == 16)
 					cp_async16(dst, in + (bo | soff[r]));
 				else
@@ -472,7 +469,7 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 			for (int h = 0; h < VT; ++h)
 #pragma unroll
 				for (int r = 0; r < NA; ++r)
-					insq += sqabs(tile[stid[h] ^ sro[r]]);
+					insq += sqabs(tile[stid(h) ^ sro[r]]);
 			__syncthreads();
 		}
 		for (int p = 0; p < npass; ++p) {
@@ -617,14 +614,14 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 			C2 a[NA];
 #pragma unroll
 			for (int r = 0; r < NA; ++r)
-				a[r] = tile[stid[0] ^ sro[r]];
+				a[r] = tile[stid(0) ^ sro[r]];
 			__syncthreads(); /* the buffer is free */
 			if (NBUF == 1) {
 				tn = next_tile(t + gridDim.x);
 				if (tn < ntiles)
 					prefetch(tile_base(tn), bufs);
 			}
-			const uint64_t bo = base | off_t[0];
+			const uint64_t bo = base | off_t(0);
 #pragma unroll
 			for (int r = 0; r < NA; ++r) {
 				outsq += sqabs(a[r]);
@@ -634,10 +631,10 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 			/* two column sets: stream each amplitude out as it is read */
 #pragma unroll
 			for (int h = 0; h < VT; ++h) {
-				const uint64_t bo = base | off_t[h];
+				const uint64_t bo = base | off_t(h);
 #pragma unroll
 				for (int r = 0; r < NA; ++r) {
-					const C2 v = tile[stid[h] ^ sro[r]];
+					const C2 v = tile[stid(h) ^ sro[r]];
 					outsq += sqabs(v);
 					__stcs(out + (bo | soff[r]), v);
 				}

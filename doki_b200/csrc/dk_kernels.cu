@@ -247,12 +247,6 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 
 /* ---- tensor-core sweep --------------------------------------------------- */
 
-#ifndef DK_TC_SHAPE
-#define DK_TC_SHAPE 4
-#endif
-#ifndef DK_TC_NBUF
-#define DK_TC_NBUF 1
-#endif
 #ifndef DK_TC_MINB11
 #define DK_TC_MINB11 3
 #endif
@@ -268,18 +262,6 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 	asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
 	    : "+d"(d0), "+d"(d1)
 	    : "d"(a), "d"(b));
-}
-
-/* FP64 tensor-core MMA, D (16x8) += A (16x16, row-major) * B (16x8,
- * column-major), with g = l/4, t = l%4: lane l holds A[g + 8(i%2)][t + 4(i/2)]
- * (i < 8), B[t + 4i][g] (i < 4) and D[g + 8(i/2)][2t + i%2] (i < 4). */
-__device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], const double (&b)[4])
-{
-	asm("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, "
-	    "{%4, %5, %6, %7, %8, %9, %10, %11}, {%12, %13, %14, %15}, {%0, %1, %2, %3};\n"
-	    : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-	    : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]),
-	      "d"(a[7]), "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 /* Sweep whose gate list holds only 8x8 matrices in register order (folded
@@ -328,7 +310,7 @@ __device__ __forceinline__ void tc_product(const double2 &e0, const double2 &e1,
 	y[3] = p3[1] - p1[1] - p2[1];
 }
 
-template <typename R, int SW, int M, int MINB, int NBUF>
+template <typename R, int SW, int M, int MINB>
 __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 	k_sweep_tc(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
 		   const unsigned char *__restrict__ prog, double *partials)
@@ -346,7 +328,7 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 	const int ncond = (int)h->ncond;
 	const size_t gate_bytes = (size_t)ngate * sizeof(dk_gate_desc);
 	C2 *const bufs = reinterpret_cast<C2 *>(sm);
-	uint4 *sg = reinterpret_cast<uint4 *>(sm + NBUF * sizeof(C2) * tn_amp);
+	uint4 *sg = reinterpret_cast<uint4 *>(sm + sizeof(C2) * tn_amp);
 	dk_gate_cond *scond =
 		reinterpret_cast<dk_gate_cond *>(reinterpret_cast<unsigned char *>(sg) + gate_bytes);
 	const dk_pass_desc *passes = reinterpret_cast<const dk_pass_desc *>(prog + h->pass_off);
@@ -443,23 +425,11 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 	if (t < ntiles)
 		prefetch(tile_base(t), bufs);
 	const uint32_t gl = lane >> 2, gk = lane & 3u;
-	int cur = 0;
 	while (t < ntiles) {
 		const uint64_t base = tile_base(t);
-		C2 *const tile = bufs + (NBUF == 2 ? cur * tn_amp : 0);
+		C2 *const tile = bufs;
 		uint64_t tn = ntiles;
-		if (NBUF == 2) {
-			/* the next tile streams into the other buffer meanwhile */
-			tn = next_tile(t + gridDim.x);
-			if (tn < ntiles) {
-				prefetch(tile_base(tn), bufs + (cur ^ 1) * tn_amp);
-				asm volatile("cp.async.wait_group 1;\n" ::);
-			} else {
-				cp_async_wait_all();
-			}
-		} else {
-			cp_async_wait_all();
-		}
+		cp_async_wait_all();
 		__syncthreads();
 		if (skip_idle) {
 			/* only touched tiles reach here: their old |amp|^2 leaves csq.
@@ -546,22 +516,10 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 					if (((base & c.gc) != c.gc) || (base & c.ga))
 						continue;
 				}
-				const uint32_t code = d.x & 0xffffu;
-				uint32_t mi = d.x >> 16; /* whole 8x8 matrices */
-				if (code == DK_GC_DENSE3V) {
-					/* the tile's conditions pick one of 2^d.w products */
-					for (uint32_t c = 0; c < d.w; ++c) {
-						const dk_gate_cond cc = scond[(d.z >> (10 * c)) & 1023u];
-						if (((base & cc.gc) == cc.gc) && !(base & cc.ga))
-							mi += 1u << c;
-					}
-				}
-				const double2 *mt = mats + 64 * (size_t)mi + 8 * gl + gk;
+				/* lane fragments: entries (l/4, l%4) and (l/4, 4 + l%4) */
+				const double2 *mt = mats + 64 * (size_t)tc_matrix(d, scond, base) + 8 * gl + gk;
 				const double2 e0 = __ldg(mt), e1 = __ldg(mt + 4);
-#if DK_TC_SHAPE == 16
-				const double wa[8] = { e0.x, e0.y, e1.x, e1.y, -e0.y, e0.x, -e1.y, e1.x };
-#endif
-				const bool ctl = code == DK_GC_DENSE3 + 1;
+				const bool ctl = (d.x & 0xffffu) == DK_GC_DENSE3 + 1;
 				/* one column group at a time: the groups' slots are
 				 * disjoint */
 #pragma unroll
@@ -572,24 +530,8 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 					const uint32_t bg = sgl ^ ((q & 1) ? t8 : 0u) ^ ((q & 2) ? t16 : 0u);
 					const double2 x0 = to_c128(tile[bg ^ gj0]);
 					const double2 x1 = to_c128(tile[bg ^ gj1]);
-					double y[4] = { 0.0, 0.0, 0.0, 0.0 };
-#if DK_TC_SHAPE == 16
-					dmma16(y, wa, { x0.x, x1.x, x0.y, x1.y });
-#else
-					/* Gauss: Mr xr, Mi xi and (Mr + Mi)(xr + xi), three real
-					 * 8x8 products of two k-steps each */
-					double p1[2] = { 0.0, 0.0 }, p2[2] = { 0.0, 0.0 }, p3[2] = { 0.0, 0.0 };
-					dmma(p1[0], p1[1], e0.x, x0.x);
-					dmma(p2[0], p2[1], e0.y, x0.y);
-					dmma(p3[0], p3[1], e0.x + e0.y, x0.x + x0.y);
-					dmma(p1[0], p1[1], e1.x, x1.x);
-					dmma(p2[0], p2[1], e1.y, x1.y);
-					dmma(p3[0], p3[1], e1.x + e1.y, x1.x + x1.y);
-					y[0] = p1[0] - p2[0];
-					y[1] = p1[1] - p2[1];
-					y[2] = p3[0] - p1[0] - p2[0];
-					y[3] = p3[1] - p1[1] - p2[1];
-#endif
+					double y[4];
+					tc_product(e0, e1, x0, x1, y);
 					__syncwarp(); /* the group's gathers precede its writes */
 #pragma unroll
 					for (int e = 0; e < 2; ++e) {
@@ -616,11 +558,9 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 			for (int r = 0; r < NA; ++r)
 				a[r] = tile[stid(0) ^ sro[r]];
 			__syncthreads(); /* the buffer is free */
-			if (NBUF == 1) {
-				tn = next_tile(t + gridDim.x);
-				if (tn < ntiles)
-					prefetch(tile_base(tn), bufs);
-			}
+			tn = next_tile(t + gridDim.x);
+			if (tn < ntiles)
+				prefetch(tile_base(tn), bufs);
 			const uint64_t bo = base | off_t(0);
 #pragma unroll
 			for (int r = 0; r < NA; ++r) {
@@ -640,14 +580,11 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 				}
 			}
 			__syncthreads(); /* the buffer is free */
-			if (NBUF == 1) {
-				tn = next_tile(t + gridDim.x);
-				if (tn < ntiles)
-					prefetch(tile_base(tn), bufs);
-			}
+			tn = next_tile(t + gridDim.x);
+			if (tn < ntiles)
+				prefetch(tile_base(tn), bufs);
 		}
 		t = tn;
-		cur ^= 1;
 	}
 	cp_async_wait_all();
 	block_sum2(insq, outsq);
@@ -1514,16 +1451,16 @@ static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dpr
 	return cudaGetLastError();
 }
 
-template <typename R, int SW, int M, int MINB, int NBUF>
+template <typename R, int SW, int M, int MINB>
 static cudaError_t run_sweep_tc(const void *in, void *out, const unsigned char *dprog,
 				const dk_sweep_hdr *hp, int num_sms, const Scratch &s,
 				cudaStream_t st, int *blocks_out)
 {
 	typedef typename CT<R>::T C2;
 	const int m = hp->m;
-	const size_t smem = NBUF * (sizeof(C2) << m) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
+	const size_t smem = (sizeof(C2) << m) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
 			    (size_t)hp->ncond * sizeof(dk_gate_cond);
-	auto kern = k_sweep_tc<R, SW, M, MINB, NBUF>;
+	auto kern = k_sweep_tc<R, SW, M, MINB>;
 	/* raised once to the device maximum, never lowered (see run_sweep) */
 	static std::once_flag once;
 	static cudaError_t set_err = cudaSuccess;
@@ -1565,14 +1502,14 @@ cudaError_t launch_sweep(int prec, const void *in, void *out,
 	if (hp->mode == DK_SWEEP_TENSOR) {
 		/* FP64 tensor-core passes; tiles of 8 to 12 bits */
 		if (prec == DK_C128)
-			e = m >= 12 ? run_sweep_tc<double, 3, 12, DK_TC_MINB12, 1>(in, out, dprog, hp,
+			e = m >= 12 ? run_sweep_tc<double, 3, 12, DK_TC_MINB12>(in, out, dprog, hp,
 										num_sms, s, st, &blocks)
-				    : run_sweep_tc<double, 3, 11, DK_TC_MINB11, DK_TC_NBUF>(in, out, dprog, hp,
+				    : run_sweep_tc<double, 3, 11, DK_TC_MINB11>(in, out, dprog, hp,
 										num_sms, s, st, &blocks);
 		else
-			e = m >= 12 ? run_sweep_tc<float, 4, 12, DK_TC_MINB12, 1>(in, out, dprog, hp,
+			e = m >= 12 ? run_sweep_tc<float, 4, 12, DK_TC_MINB12>(in, out, dprog, hp,
 									       num_sms, s, st, &blocks)
-				    : run_sweep_tc<float, 4, 11, DK_TC_MINB11, DK_TC_NBUF>(in, out, dprog, hp,
+				    : run_sweep_tc<float, 4, 11, DK_TC_MINB11>(in, out, dprog, hp,
 									       num_sms, s, st, &blocks);
 		if (e != cudaSuccess)
 			return e;

@@ -26,7 +26,7 @@
 
 namespace {
 
-/* A slot: one CUDA stream with its own scratch and cuBLAS handle.  Every
+/* A slot: one CUDA stream with its own scratch and lock.  Every
  * register belongs to the slot that created it (derived registers inherit
  * it); work on a register is queued on its slot's stream under its slot's
  * lock, so registers of different slots run concurrently on the device and a

@@ -1125,11 +1125,12 @@ __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, b
 /* One lower 64x64 tile (ti >= tj) per CTA and one traced chunk per grid row.
  * 8 warps as 2 x 4: a warp owns rows 32 wr .. +32 (4 MMA row blocks) and
  * columns 16 wc .. +16 (2 column blocks).  Per 4 traced values (one k-step)
- * each 8x8 block takes 4 FP64 MMAs:
- *   re += Xr Xr'^T + Xi Xi'^T,  im += Xi Xr'^T - Xr Xi'^T.
+ * each 8x8 block takes 3 FP64 MMAs (Gauss): P1 += Xr Xr'^T, P2 += Xi Xi'^T,
+ * P3 += (Xr + Xi)(Xr' - Xi')^T; re = P1 + P2, im = P3 - P1 + P2.  The 24
+ * accumulators of a lane need one CTA per SM. 
  * Slabs are stored [b][a ^ 2 (b & 3)] so a quarter-warp's fragment reads
  * (4 traced rows x 2 columns) hit 8 distinct 16-byte bank groups. */
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, 1)
 	k_rho_tc(const double2 *__restrict__ A, uint64_t dim, uint64_t K, uint64_t bchunk,
 		 double2 *part, double alpha)
 {
@@ -1170,13 +1171,13 @@ __global__ void __launch_bounds__(256, 2)
 		cp_async_commit();
 	};
 
-	double acc[4][2][4];
+	double acc[4][2][6]; /* Gauss: Xr Xr', Xi Xi', (Xr + Xi)(Xr' - Xi') */
 #pragma unroll
 	for (int i = 0; i < 4; ++i)
 #pragma unroll
 		for (int j = 0; j < 2; ++j)
 #pragma unroll
-			for (int v = 0; v < 4; ++v)
+			for (int v = 0; v < 6; ++v)
 				acc[i][j][v] = 0.0;
 
 	const int bsel = diag ? 0 : 1;
@@ -1207,9 +1208,8 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
 				for (int j = 0; j < 2; ++j) {
 					dmma(acc[i][j][0], acc[i][j][1], xa[i].x, xb[j].x);
-					dmma(acc[i][j][0], acc[i][j][1], xa[i].y, xb[j].y);
-					dmma(acc[i][j][2], acc[i][j][3], xa[i].y, xb[j].x);
-					dmma(acc[i][j][2], acc[i][j][3], -xa[i].x, xb[j].y);
+					dmma(acc[i][j][2], acc[i][j][3], xa[i].y, xb[j].y);
+					dmma(acc[i][j][4], acc[i][j][5], xa[i].x + xa[i].y, xb[j].x - xb[j].y);
 				}
 		}
 		__syncthreads(); /* this buffer is refilled two slabs later */
@@ -1225,7 +1225,8 @@ __global__ void __launch_bounds__(256, 2)
 			for (int e = 0; e < 2; ++e) {
 				const uint64_t a = a0 + 32u * wr + 8u * i + g;
 				const uint64_t c = c0 + 16u * wc + 8u * j + 2u * t + e;
-				P[a + c * dim] = make_double2(f * acc[i][j][e], f * acc[i][j][2 + e]);
+				const double p1 = acc[i][j][e], p2 = acc[i][j][2 + e], p3 = acc[i][j][4 + e];
+				P[a + c * dim] = make_double2(f * (p1 + p2), f * (p3 - p1 + p2));
 			}
 }
 

@@ -7,15 +7,20 @@
  * exception object (qsimov.doki.error) and error strings as the reference
  * binding.  Differences, all strictly safer: out-of-range ids (registry_get,
  * registry_prob, funmatrix_partialtrace) and repeated targets raise instead
- * of reading out of bounds, and a registry passed to registry_del raises on
- * later use instead of being a dangling pointer.
+ * of reading out of bounds; a registry passed to registry_del raises on
+ * later use instead of being a dangling pointer; custom matrices of any shape
+ * are stored row-major (the reference indexes them with the row count);
+ * funmatrix_projection and funmatrix_apply honour their qubit id and state
+ * arguments (the reference's wrappers store "p" ints into 1-byte bools next
+ * to them).
  *
  * Extensions (optional trailing arguments never break positional calls):
  *   registry_new(n, verbose[, precision]) / registry_new_data(n, values,
  *   verbose[, precision]) -- precision 2 = complex128 (default), 1 = complex64;
  *   registry_get_all(reg, canonical) -> numpy complex128 array;
  *   registry_probs(reg) -> list of all P(q = 1);
- *   funmatrix_numpy(fm) -> numpy array of a density / reduced density matrix;
+ *   funmatrix_numpy(fm) -> numpy array of any functional matrix (one device
+ *   call for a reduced density matrix);
  *   registry_precision(reg); registry_flush(reg); registry_compare(a, b);
  *   engine_sync();
  *   engine_set_fusion(bool); engine_stats(); engine_stream();
@@ -86,6 +91,9 @@ static PyObject *wrap_state(dk_state *s)
 
 /* ======================= functional matrices ============================ */
 
+/* Node kinds.  Every node carries the reference's per-node modifiers
+ * (funmatrix.h struct FMatrix): a scalar s, a transpose flag and a conjugate
+ * flag, applied by fmat_get around the kind's own element rule. */
 enum {
 	FM_CUSTOM = 1,
 	FM_IDENTITY,
@@ -95,20 +103,75 @@ enum {
 	FM_CU,
 	FM_DENSITY,
 	FM_PTRACE,
+	FM_EYEKRON,
+	FM_PROJECTION,
+	FM_APPLY,
+	/* operation nodes A op B (funmatrix.h op codes 0-4) */
+	FM_ADD,
+	FM_SUB,
+	FM_MATMUL,
+	FM_EWMUL,
+	FM_KRON,
 };
+
+/* Element status codes of the reference's getitem (funmatrix.c:238-340),
+ * offset by 100 so they never collide with DK_* codes. */
+enum {
+	FMG_ADD = 101,
+	FMG_SUB,
+	FMG_MATMUL,
+	FMG_EWMUL,
+	FMG_KRON,
+	FMG_OP,
+	FMG_BOUNDS,
+	FMG_NAN,
+};
+
+/* Host array of a custom matrix, shared by the copies that scalar products,
+ * transposes and daggers make. */
+typedef struct fm_buf {
+	size_t refs;
+	size_t len;
+	double complex v[];
+} fm_buf;
 
 typedef struct fmat {
 	int kind;
 	uint64_t r, c;
-	PyObject *parent; /* state capsule (DENSITY) / funmatrix capsule (CU, PTRACE) */
-	int elem; /* PTRACE: qubit traced out of the parent */
+	double complex s;
+	int transpose, conjugate;
+	/* A and B of operation nodes; the operand of CU, PTRACE, EYEKRON and
+	 * PROJECTION (a); state and gate of APPLY; the state capsule of DENSITY */
+	PyObject *a, *b;
+	int elem; /* PTRACE: traced qubit; PROJECTION: qubit id */
+	int value; /* PROJECTION: kept value of the qubit */
+	uint64_t left, right; /* EYEKRON: identity sizes 2^leftQ, 2^rightQ */
 	int hadamard;
-	double complex *data; /* CUSTOM, row-major r x c */
+	fm_buf *data; /* CUSTOM, row-major r x c */
+	unsigned *targets; /* APPLY */
+	unsigned ntargets;
+	uint64_t cmask, amask;
 	/* PTRACE chains rooted at a register: materialised reduced density */
 	int mat_ready;
 	uint64_t keep_mask;
 	double complex *rho;
 } fmat;
+
+static void fm_buf_release(fm_buf *b)
+{
+	if (b && --b->refs == 0)
+		free(b);
+}
+
+static void fmat_free(fmat *m)
+{
+	Py_XDECREF(m->a);
+	Py_XDECREF(m->b);
+	fm_buf_release(m->data);
+	free(m->targets);
+	free(m->rho);
+	free(m);
+}
 
 static void fmat_destroy(PyObject *cap)
 {
@@ -117,20 +180,14 @@ static void fmat_destroy(PyObject *cap)
 		PyErr_Clear();
 		return;
 	}
-	Py_XDECREF(m->parent);
-	free(m->data);
-	free(m->rho);
-	free(m);
+	fmat_free(m);
 }
 
 static PyObject *wrap_fmat(fmat *m)
 {
 	PyObject *c = PyCapsule_New(m, CAP_FMAT, fmat_destroy);
-	if (!c) {
-		Py_XDECREF(m->parent);
-		free(m->data);
-		free(m);
-	}
+	if (!c)
+		fmat_free(m);
 	return c;
 }
 
@@ -141,8 +198,59 @@ static fmat *fmat_new(int kind, uint64_t r, uint64_t c)
 		m->kind = kind;
 		m->r = r;
 		m->c = c;
+		m->s = 1.0;
 	}
 	return m;
+}
+
+/* A node that evaluates like m with its own modifiers (mprod, mdiv,
+ * transpose and dagger, funmatrix.c:428-860): operands and custom data are
+ * shared, the reduced-density cache is not. */
+static fmat *fmat_copy(const fmat *m)
+{
+	fmat *d = fmat_new(m->kind, m->r, m->c);
+	if (!d)
+		return NULL;
+	if (m->targets) {
+		d->targets = (unsigned *)malloc(sizeof(unsigned) * (m->ntargets ? m->ntargets : 1));
+		if (!d->targets) {
+			free(d);
+			return NULL;
+		}
+		memcpy(d->targets, m->targets, sizeof(unsigned) * m->ntargets);
+	}
+	d->s = m->s;
+	d->transpose = m->transpose;
+	d->conjugate = m->conjugate;
+	d->a = m->a;
+	Py_XINCREF(d->a);
+	d->b = m->b;
+	Py_XINCREF(d->b);
+	d->elem = m->elem;
+	d->value = m->value;
+	d->left = m->left;
+	d->right = m->right;
+	d->hadamard = m->hadamard;
+	d->data = m->data;
+	if (d->data)
+		d->data->refs++;
+	d->ntargets = m->ntargets;
+	d->cmask = m->cmask;
+	d->amask = m->amask;
+	return d;
+}
+
+static fmat *fmat_of(PyObject *cap)
+{
+	fmat *m = cap ? (fmat *)PyCapsule_GetPointer(cap, CAP_FMAT) : NULL;
+	if (!m)
+		PyErr_Clear();
+	return m;
+}
+
+static int fmat_plain(const fmat *m)
+{
+	return m->s == 1.0 && !m->transpose && !m->conjugate;
 }
 
 static uint64_t ins_bit(uint64_t pos, int e, int v)
@@ -155,28 +263,27 @@ static uint64_t ins_bit(uint64_t pos, int e, int v)
 static int ilog2(uint64_t x)
 {
 	int l = 0;
-	while ((1ull << l) < x)
+	while (l < 64 && (1ull << l) < x)
 		l++;
 	return l;
 }
 
-/* If the chain of partial traces ends at a register's density matrix,
- * return its state capsule and the surviving-qubit mask. */
+/* If the chain of partial traces below m ends at a register's density
+ * matrix and no node on the way carries a modifier, return the state
+ * capsule and the surviving-qubit mask. */
 static PyObject *ptrace_root(fmat *m, uint64_t *keep)
 {
 	int elems[64], ne = 0;
 	fmat *cur = m;
 	while (cur->kind == FM_PTRACE && ne < 64) {
 		elems[ne++] = cur->elem;
-		cur = (fmat *)PyCapsule_GetPointer(cur->parent, CAP_FMAT);
-		if (!cur) {
-			PyErr_Clear();
+		cur = fmat_of(cur->a);
+		if (!cur || !fmat_plain(cur))
 			return NULL;
-		}
 	}
 	if (cur->kind != FM_DENSITY)
 		return NULL;
-	dk_state *s = (dk_state *)PyCapsule_GetPointer(cur->parent, CAP_STATE);
+	dk_state *s = (dk_state *)PyCapsule_GetPointer(cur->a, CAP_STATE);
 	if (!s) {
 		PyErr_Clear();
 		return NULL;
@@ -198,15 +305,48 @@ static PyObject *ptrace_root(fmat *m, uint64_t *keep)
 	for (int i = 0; i < na; i++)
 		k |= 1ull << alive[i];
 	*keep = k;
-	return cur->parent;
+	return cur->a;
 }
 
-/* Element (i, j); returns 0 or a DK status (Python error not set). */
-static int fmat_get(fmat *m, uint64_t i, uint64_t j, double complex *out)
+static int fmat_get(fmat *m, uint64_t i, uint64_t j, double complex *out);
+
+/* A child element inside a functional node: a failing child makes the node's
+ * value NaN in the reference (its getitem leaves NaN behind), which the
+ * caller reports as FMG_NAN; engine errors pass through. */
+static int child_get(PyObject *cap, uint64_t i, uint64_t j, double complex *out)
 {
+	fmat *c = fmat_of(cap);
+	if (!c)
+		return FMG_NAN;
+	int rc = fmat_get(c, i, j, out);
+	return rc >= FMG_ADD ? FMG_NAN : rc;
+}
+
+/* Two operand elements of an operation node; any operand failure becomes
+ * the node's own code. */
+static int op_get(fmat *m, uint64_t ia, uint64_t ja, uint64_t ib, uint64_t jb,
+		  double complex *x, double complex *y, int code)
+{
+	fmat *A = fmat_of(m->a), *B = fmat_of(m->b);
+	if (!A || !B)
+		return code;
+	int r1 = fmat_get(A, ia, ja, x);
+	int r2 = fmat_get(B, ib, jb, y);
+	if (r1 && r1 < FMG_ADD)
+		return r1;
+	if (r2 && r2 < FMG_ADD)
+		return r2;
+	return (r1 || r2) ? code : 0;
+}
+
+/* The kind's element rule at (i, j), after the node's transpose swap. */
+static int fmat_elem(fmat *m, uint64_t i, uint64_t j, double complex *out)
+{
+	double complex x, y;
+	int rc;
 	switch (m->kind) {
 	case FM_CUSTOM:
-		*out = m->data[i * m->c + j];
+		*out = m->data->v[i * m->c + j];
 		return 0;
 	case FM_IDENTITY:
 		*out = (i == j) ? 1.0 : 0.0;
@@ -227,26 +367,24 @@ static int fmat_get(fmat *m, uint64_t i, uint64_t j, double complex *out)
 	}
 	case FM_CU: {
 		/* funmatrix.c:1194-1219: identity block, then U in the last block */
-		fmat *u = (fmat *)PyCapsule_GetPointer(m->parent, CAP_FMAT);
-		if (!u) {
-			PyErr_Clear();
-			return DK_ERR_ARG;
-		}
+		fmat *u = fmat_of(m->a);
+		if (!u)
+			return FMG_NAN;
 		if (i < u->r || j < u->c) {
 			*out = (i == j) ? 1.0 : 0.0;
 			return 0;
 		}
-		return fmat_get(u, i - u->r, j - u->c, out);
+		return child_get(m->a, i - u->r, j - u->c, out);
 	}
 	case FM_DENSITY: {
 		/* qops.c:266-293: psi_i conj(psi_j) */
-		dk_state *s = (dk_state *)PyCapsule_GetPointer(m->parent, CAP_STATE);
+		dk_state *s = (dk_state *)PyCapsule_GetPointer(m->a, CAP_STATE);
 		if (!s) {
 			PyErr_Clear();
 			return DK_ERR_ARG;
 		}
 		double ar, ai, br, bi;
-		int rc = dk_get_amplitude(s, i, &ar, &ai);
+		rc = dk_get_amplitude(s, i, &ar, &ai);
 		if (!rc)
 			rc = dk_get_amplitude(s, j, &br, &bi);
 		if (rc)
@@ -270,7 +408,7 @@ static int fmat_get(fmat *m, uint64_t i, uint64_t j, double complex *out)
 					(double complex *)malloc(sizeof(double complex) * dim * dim);
 				if (!rho)
 					return DK_ERR_ALLOC;
-				int rc = dk_reduced_density(s, keep, (double *)rho);
+				rc = dk_reduced_density(s, keep, (double *)rho);
 				if (rc) {
 					free(rho);
 					return rc;
@@ -282,31 +420,142 @@ static int fmat_get(fmat *m, uint64_t i, uint64_t j, double complex *out)
 				return 0;
 			}
 			double re, im;
-			int rc = dk_reduced_density_elem(s, keep, i, j, &re, &im);
+			rc = dk_reduced_density_elem(s, keep, i, j, &re, &im);
 			if (rc)
 				return rc;
 			*out = re + I * im;
 			return 0;
 		}
 		/* generic lazy partial trace (funmatrix.c:920-944) */
-		fmat *p = (fmat *)PyCapsule_GetPointer(m->parent, CAP_FMAT);
-		if (!p) {
-			PyErr_Clear();
-			return DK_ERR_ARG;
-		}
-		double complex a, b;
-		int rc = fmat_get(p, ins_bit(i, m->elem, 0), ins_bit(j, m->elem, 0), &a);
+		rc = child_get(m->a, ins_bit(i, m->elem, 0), ins_bit(j, m->elem, 0), &x);
+		if (!rc)
+			rc = child_get(m->a, ins_bit(i, m->elem, 1), ins_bit(j, m->elem, 1), &y);
 		if (rc)
 			return rc;
-		rc = fmat_get(p, ins_bit(i, m->elem, 1), ins_bit(j, m->elem, 1), &b);
-		if (rc)
-			return rc;
-		*out = a + b;
+		*out = x + y;
 		return 0;
 	}
-	default:
-		return DK_ERR_ARG;
+	case FM_EYEKRON: {
+		/* funmatrix.c:665-707: I(2^left) (x) U (x) I(2^right) */
+		fmat *u = fmat_of(m->a);
+		if (!u)
+			return FMG_NAN;
+		if (i % m->right != j % m->right) {
+			*out = 0.0;
+			return 0;
+		}
+		i /= m->right;
+		j /= m->right;
+		if (i / u->r != j / u->c) {
+			*out = 0.0;
+			return 0;
+		}
+		return child_get(m->a, i % u->r, j % u->c, out);
 	}
+	case FM_PROJECTION: {
+		/* funmatrix.c:862-890: rows whose qubit differs from value are 0 */
+		const int bit = (i >> m->elem) & 1;
+		if (bit != m->value) {
+			*out = 0.0;
+			return 0;
+		}
+		return child_get(m->a, i, j, out);
+	}
+	case FM_APPLY: {
+		/* qops.c:498-563: controlled gate applied to a column vector */
+		if ((i & m->cmask) != m->cmask || (i & m->amask))
+			return child_get(m->a, i, 0, out);
+		fmat *g = fmat_of(m->b);
+		if (!g)
+			return FMG_NAN;
+		uint64_t row = 0, reg = i;
+		for (unsigned k = 0; k < m->ntargets; k++)
+			row |= ((i >> m->targets[k]) & 1ull) << k;
+		double complex acc = 0.0;
+		for (uint64_t n = 0; n < g->r; n++) {
+			for (unsigned k = 0; k < m->ntargets; k++) {
+				const uint64_t tb = 1ull << m->targets[k];
+				reg = ((n >> k) & 1ull) ? (reg | tb) : (reg & ~tb);
+			}
+			rc = child_get(m->a, reg, 0, &x);
+			if (!rc)
+				rc = child_get(m->b, row, n, &y);
+			if (rc)
+				return rc;
+			acc = acc + x * y;
+		}
+		*out = acc;
+		return 0;
+	}
+	case FM_ADD:
+		rc = op_get(m, i, j, i, j, &x, &y, FMG_ADD);
+		if (!rc)
+			*out = x + y;
+		return rc;
+	case FM_SUB:
+		rc = op_get(m, i, j, i, j, &x, &y, FMG_SUB);
+		if (!rc)
+			*out = x - y;
+		return rc;
+	case FM_MATMUL: {
+		fmat *A = fmat_of(m->a);
+		if (!A)
+			return FMG_MATMUL;
+		double complex acc = 0.0;
+		for (uint64_t k = 0; k < A->c; k++) {
+			rc = op_get(m, i, k, k, j, &x, &y, FMG_MATMUL);
+			if (rc)
+				return rc;
+			acc = acc + x * y;
+		}
+		*out = acc;
+		return 0;
+	}
+	case FM_EWMUL:
+		rc = op_get(m, i, j, i, j, &x, &y, FMG_EWMUL);
+		if (!rc)
+			*out = x * y;
+		return rc;
+	case FM_KRON: {
+		fmat *B = fmat_of(m->b);
+		if (!B)
+			return FMG_KRON;
+		rc = op_get(m, i / B->r, j / B->c, i % B->r, j % B->c, &x, &y, FMG_KRON);
+		if (!rc)
+			*out = x * y;
+		return rc;
+	}
+	default:
+		return FMG_OP;
+	}
+}
+
+/* Element (i, j) as the reference's getitem computes it: bounds, transpose
+ * swap, the kind's rule (NaN from a functional node is an error), conjugate,
+ * then the node's scalar.  Returns 0, an FMG_* code or a DK status (Python
+ * error not set). */
+static int fmat_get(fmat *m, uint64_t i, uint64_t j, double complex *out)
+{
+	*out = NAN;
+	if (i >= m->r || j >= m->c)
+		return FMG_BOUNDS;
+	if (m->transpose) {
+		const uint64_t t = i;
+		i = j;
+		j = t;
+	}
+	double complex v = NAN;
+	int rc = fmat_elem(m, i, j, &v);
+	if (rc)
+		return rc;
+	if (m->kind < FM_ADD && (isnan(creal(v)) || isnan(cimag(v)))) {
+		*out = v;
+		return FMG_NAN;
+	}
+	if (m->conjugate)
+		v = conj(v);
+	*out = v * m->s;
+	return 0;
 }
 
 /* ============================ gates ===================================== */
@@ -979,7 +1228,7 @@ static PyObject *doki_registry_density(PyObject *self, PyObject *args)
 		return NULL;
 	}
 	Py_INCREF(cap);
-	m->parent = cap;
+	m->a = cap;
 	return wrap_fmat(m);
 }
 
@@ -1111,6 +1360,17 @@ static fmat *get_fmat(PyObject *cap)
 	return m;
 }
 
+/* The reference raises DokiError over the capsule's own error. */
+static fmat *get_fmat_msg(PyObject *cap, const char *msg)
+{
+	fmat *m = (fmat *)PyCapsule_GetPointer(cap, CAP_FMAT);
+	if (!m) {
+		PyErr_Clear();
+		PyErr_SetString(DokiError, msg);
+	}
+	return m;
+}
+
 static PyObject *doki_funmatrix_create(PyObject *self, PyObject *args)
 {
 	PyObject *list;
@@ -1139,30 +1399,30 @@ static PyObject *doki_funmatrix_create(PyObject *self, PyObject *args)
 		return NULL;
 	}
 	fmat *m = fmat_new(FM_CUSTOM, (uint64_t)nr, (uint64_t)nc);
-	double complex *d = (double complex *)malloc(sizeof(double complex) * nr * nc);
+	fm_buf *d = (fm_buf *)malloc(sizeof(fm_buf) + sizeof(double complex) * nr * nc);
 	if (!m || !d) {
 		free(m);
 		free(d);
 		PyErr_SetString(DokiError, "failed to allocate 2D matrix");
 		return NULL;
 	}
+	d->refs = 1;
+	d->len = (size_t)(nr * nc);
+	m->data = d;
 	for (Py_ssize_t i = 0; i < nr; i++) {
 		row = PyList_GetItem(list, i);
 		if (!PyList_Check(row) || PyList_Size(row) != nc) {
-			free(m);
-			free(d);
+			fmat_free(m);
 			PyErr_SetString(DokiError, "rows must be lists of the same size");
 			return NULL;
 		}
 		for (Py_ssize_t j = 0; j < nc; j++)
-			if (py_to_complex(PyList_GetItem(row, j), &d[i * nc + j])) {
-				free(m);
-				free(d);
+			if (py_to_complex(PyList_GetItem(row, j), &d->v[i * nc + j])) {
+				fmat_free(m);
 				PyErr_SetString(DokiError, "matrix elements must be complex numbers");
 				return NULL;
 			}
 	}
-	m->data = d;
 	return wrap_fmat(m);
 }
 
@@ -1220,24 +1480,35 @@ static PyObject *doki_funmatrix_addcontrol(PyObject *self, PyObject *args)
 		PyErr_SetString(DokiError, "Syntax: funmatrix_addcontrol(funmatrix, verbose)");
 		return NULL;
 	}
-	fmat *u = (fmat *)PyCapsule_GetPointer(cap, CAP_FMAT);
-	if (!u) {
-		PyErr_SetString(DokiError, "NULL pointer to matrix");
+	fmat *u = get_fmat_msg(cap, "NULL pointer to matrix");
+	if (!u)
 		return NULL;
-	}
 	fmat *m = fmat_new(FM_CU, u->r * 2, u->c * 2);
 	if (!m) {
 		PyErr_SetString(DokiError, "NULL pointer to matrix");
 		return NULL;
 	}
 	Py_INCREF(cap);
-	m->parent = cap;
+	m->a = cap;
 	return wrap_fmat(m);
 }
 
+/* Reference getitem codes -> its messages (doki.c:1528-1570, 2155-2205). */
 static PyObject *get_error(int rc, const char *prefix)
 {
-	if (rc == DK_ERR_ARG)
+	static const char *const what[] = {
+		"Error adding parent matrices",
+		"Error substracting parent matrices",
+		"Error multiplying parent matrices",
+		"Error multiplying entity-wise parent matrices",
+		"Error calculating Kronecker product of parent matrices",
+		"Unknown operation between parent matrices",
+		"Element out of bounds",
+		"f returned NAN",
+	};
+	if (rc >= FMG_ADD && rc <= FMG_NAN)
+		PyErr_Format(DokiError, "[%s] %s", prefix, what[rc - FMG_ADD]);
+	else if (rc == DK_ERR_ARG)
 		PyErr_Format(DokiError, "[%s] Element out of bounds", prefix);
 	else
 		raise_dk(rc, prefix);
@@ -1253,7 +1524,7 @@ static PyObject *doki_funmatrix_get(PyObject *self, PyObject *args)
 		PyErr_SetString(DokiError, "Syntax: funmatrix_get(funmatrix, i, j, verbose)");
 		return NULL;
 	}
-	fmat *m = get_fmat(cap);
+	fmat *m = get_fmat_msg(cap, "NULL pointer to matrix");
 	if (!m)
 		return NULL;
 	if (i >= m->r || j >= m->c) {
@@ -1281,7 +1552,8 @@ static PyObject *doki_funmatrix_numpy(PyObject *self, PyObject *args)
 	fmat *m = get_fmat(cap);
 	if (!m)
 		return NULL;
-	if (m->r * m->c > (1ull << 28)) {
+	if (m->r == 0 || m->c == 0 || m->r > (1ull << 28) || m->c > (1ull << 28) ||
+	    m->r * m->c > (1ull << 28)) {
 		PyErr_SetString(DokiError, "matrix too large to export");
 		return NULL;
 	}
@@ -1301,10 +1573,10 @@ static PyObject *doki_funmatrix_numpy(PyObject *self, PyObject *args)
 		return NULL;
 	}
 	double complex *out = (double complex *)view.buf;
-	if (m->kind == FM_PTRACE && m->mat_ready)
+	if (m->kind == FM_PTRACE && m->mat_ready && fmat_plain(m))
 		memcpy(out, m->rho, sizeof(double complex) * m->r * m->c);
-	else if (m->kind == FM_CUSTOM)
-		memcpy(out, m->data, sizeof(double complex) * m->r * m->c);
+	else if (m->kind == FM_CUSTOM && fmat_plain(m))
+		memcpy(out, m->data->v, sizeof(double complex) * m->r * m->c);
 	else {
 		for (uint64_t i = 0; i < m->r && !rc; i++)
 			for (uint64_t j = 0; j < m->c && !rc; j++)
@@ -1326,7 +1598,7 @@ static PyObject *doki_funmatrix_shape(PyObject *self, PyObject *args)
 		PyErr_SetString(DokiError, "Syntax: funmatrix_shape(funmatrix, verbose)");
 		return NULL;
 	}
-	fmat *m = get_fmat(cap);
+	fmat *m = get_fmat_msg(cap, "NULL pointer to matrix");
 	if (!m)
 		return NULL;
 	return Py_BuildValue("(KK)", (unsigned long long)m->r, (unsigned long long)m->c);
@@ -1341,11 +1613,9 @@ static PyObject *doki_funmatrix_partialtrace(PyObject *self, PyObject *args)
 		PyErr_SetString(DokiError, "Syntax: funmatrix_partialtrace(funmatrix, id, verbose)");
 		return NULL;
 	}
-	fmat *p = (fmat *)PyCapsule_GetPointer(cap, CAP_FMAT);
-	if (!p) {
-		PyErr_SetString(DokiError, "[PTRACE] The matrix is NULL");
+	fmat *p = get_fmat_msg(cap, "[PTRACE] The matrix is NULL");
+	if (!p)
 		return NULL;
-	}
 	if (p->r != p->c) {
 		PyErr_SetString(DokiError, "[PTRACE] The matrix is not a square matrix");
 		return NULL;
@@ -1365,7 +1635,7 @@ static PyObject *doki_funmatrix_partialtrace(PyObject *self, PyObject *args)
 	}
 	m->elem = (int)id;
 	Py_INCREF(cap);
-	m->parent = cap;
+	m->a = cap;
 	return wrap_fmat(m);
 }
 
@@ -1377,7 +1647,7 @@ static PyObject *doki_funmatrix_trace(PyObject *self, PyObject *args)
 		PyErr_SetString(DokiError, "Syntax: funmatrix_trace(funmatrix, verbose)");
 		return NULL;
 	}
-	fmat *m = get_fmat(cap);
+	fmat *m = get_fmat_msg(cap, "NULL pointer to matrix");
 	if (!m)
 		return NULL;
 	const uint64_t mn = m->r <= m->c ? m->r : m->c;
@@ -1396,13 +1666,23 @@ static PyObject *doki_funmatrix_trace(PyObject *self, PyObject *args)
 	return PyComplex_FromDoubles(creal(acc), cimag(acc));
 }
 
-static size_t fmat_mem(fmat *m)
+/* Bytes held by a node and the nodes it references (funmatrix.c:1550-1567
+ * counts operands recursively). */
+static size_t fmat_mem(fmat *m, int depth)
 {
 	size_t s = sizeof(fmat);
 	if (m->data)
-		s += sizeof(double complex) * m->r * m->c;
+		s += sizeof(fm_buf) + sizeof(double complex) * m->data->len;
 	if (m->rho)
 		s += sizeof(double complex) * m->r * m->r;
+	s += sizeof(unsigned) * m->ntargets;
+	if (depth < 256) {
+		fmat *a = fmat_of(m->a), *b = fmat_of(m->b);
+		if (a && m->kind != FM_DENSITY)
+			s += fmat_mem(a, depth + 1);
+		if (b)
+			s += fmat_mem(b, depth + 1);
+	}
 	return s;
 }
 
@@ -1414,34 +1694,459 @@ static PyObject *doki_funmatrix_mem(PyObject *self, PyObject *args)
 		PyErr_SetString(DokiError, "Syntax: funmatrix_mem(fmatrix, verbose)");
 		return NULL;
 	}
-	fmat *m = (fmat *)PyCapsule_GetPointer(cap, CAP_FMAT);
-	if (!m) {
-		PyErr_SetString(DokiError, "NULL pointer to FMatrix");
+	fmat *m = get_fmat_msg(cap, "NULL pointer to FMatrix");
+	if (!m)
 		return NULL;
-	}
-	return PyLong_FromSize_t(fmat_mem(m));
+	return PyLong_FromSize_t(fmat_mem(m, 0));
 }
 
-/* Lazy FMatrix algebra (reference funmatrix.c:343-903) and funmatrix_apply
- * (qops.c:449-563) are outside this engine's scope. */
-#define UNSUPPORTED(name)                                                          \
-	static PyObject *doki_##name(PyObject *self, PyObject *args)               \
-	{                                                                          \
-		PyErr_SetString(DokiError, #name " is not supported by this engine"); \
-		return NULL;                                                       \
+/* ---- lazy algebra (funmatrix.c:343-903, wrappers doki.c:1581-2055) ----- */
+
+/* A op B node after the reference's operand checks; errors use its
+ * "[TAG] ..." strings. */
+static PyObject *fm_binary(PyObject *args, const char *syntax, const char *tag, int kind)
+{
+	PyObject *c1, *c2;
+	int verbose;
+	if (!PyArg_ParseTuple(args, "OOp", &c1, &c2, &verbose)) {
+		PyErr_SetString(DokiError, syntax);
+		return NULL;
 	}
-UNSUPPORTED(funmatrix_add)
-UNSUPPORTED(funmatrix_sub)
-UNSUPPORTED(funmatrix_scalar_mul)
-UNSUPPORTED(funmatrix_scalar_div)
-UNSUPPORTED(funmatrix_matmul)
-UNSUPPORTED(funmatrix_ewmul)
-UNSUPPORTED(funmatrix_kron)
-UNSUPPORTED(funmatrix_eyekron)
-UNSUPPORTED(funmatrix_transpose)
-UNSUPPORTED(funmatrix_dagger)
-UNSUPPORTED(funmatrix_projection)
-UNSUPPORTED(funmatrix_apply)
+	fmat *a = (fmat *)PyCapsule_GetPointer(c1, CAP_FMAT);
+	if (!a) {
+		PyErr_Clear();
+		PyErr_Format(DokiError, "[%s] The first operand is NULL", tag);
+		return NULL;
+	}
+	fmat *b = (fmat *)PyCapsule_GetPointer(c2, CAP_FMAT);
+	if (!b) {
+		PyErr_Clear();
+		PyErr_Format(DokiError, "[%s] The second operand is NULL", tag);
+		return NULL;
+	}
+	uint64_t r, c;
+	switch (kind) {
+	case FM_ADD:
+	case FM_SUB:
+		if (a->r != b->r || a->c != b->c)
+			goto misaligned;
+		r = a->r;
+		c = a->c;
+		break;
+	case FM_EWMUL:
+		if (a->r == b->r && a->c == b->c) {
+			r = a->r;
+			c = a->c;
+		} else if (a->r == 1 && b->c == 1) {
+			/* row .* column is the outer product column * row */
+			PyObject *t = c1;
+			c1 = c2;
+			c2 = t;
+			kind = FM_MATMUL;
+			r = b->r;
+			c = a->c;
+		} else if (b->r == 1 && a->c == 1) {
+			kind = FM_MATMUL;
+			r = a->r;
+			c = b->c;
+		} else {
+			goto misaligned;
+		}
+		break;
+	case FM_MATMUL:
+		if (a->c != b->r)
+			goto misaligned;
+		r = a->r;
+		c = b->c;
+		break;
+	default: /* FM_KRON */
+		if ((a->r && b->r > UINT64_MAX / a->r) || (a->c && b->c > UINT64_MAX / a->c)) {
+			PyErr_Format(DokiError, "[%s] Failed to allocate result matrix", tag);
+			return NULL;
+		}
+		r = a->r * b->r;
+		c = a->c * b->c;
+		break;
+	}
+	fmat *m = fmat_new(kind, r, c);
+	if (!m) {
+		PyErr_Format(DokiError, "[%s] Failed to allocate result matrix", tag);
+		return NULL;
+	}
+	Py_INCREF(c1);
+	m->a = c1;
+	Py_INCREF(c2);
+	m->b = c2;
+	return wrap_fmat(m);
+misaligned:
+	PyErr_Format(DokiError, "[%s] The operands are misalligned", tag);
+	return NULL;
+}
+
+static PyObject *doki_funmatrix_add(PyObject *self, PyObject *args)
+{
+	return fm_binary(args, "Syntax: funmatrix_add(funmatrix1, funmatrix2, verbose)", "ADD",
+			 FM_ADD);
+}
+
+static PyObject *doki_funmatrix_sub(PyObject *self, PyObject *args)
+{
+	return fm_binary(args, "Syntax: funmatrix_sub(funmatrix1, funmatrix2, verbose)", "SUB",
+			 FM_SUB);
+}
+
+static PyObject *doki_funmatrix_matmul(PyObject *self, PyObject *args)
+{
+	return fm_binary(args, "Syntax: funmatrix_matmul(funmatrix1, funmatrix2, verbose)",
+			 "MATMUL", FM_MATMUL);
+}
+
+static PyObject *doki_funmatrix_ewmul(PyObject *self, PyObject *args)
+{
+	return fm_binary(args, "Syntax: funmatrix_ewmul(funmatrix1, funmatrix2, verbose)",
+			 "EWMUL", FM_EWMUL);
+}
+
+static PyObject *doki_funmatrix_kron(PyObject *self, PyObject *args)
+{
+	return fm_binary(args, "Syntax: funmatrix_kron(funmatrix1, funmatrix2, verbose)", "KRON",
+			 FM_KRON);
+}
+
+/* Copy of a node with new modifiers: scalar product / division, transpose,
+ * dagger.  The dagger flips both flags and leaves the scalar as it is, as
+ * the reference's does. */
+static PyObject *fm_modified(PyObject *cap, const char *tag, int op, double complex z)
+{
+	fmat *src = (fmat *)PyCapsule_GetPointer(cap, CAP_FMAT);
+	if (!src) {
+		PyErr_Clear();
+		PyErr_Format(DokiError, op == 'T' || op == 'H' ? "[%s] The matrix is NULL" :
+								   "[%s] The matrix operand is NULL",
+			     tag);
+		return NULL;
+	}
+	fmat *m = fmat_copy(src);
+	if (!m) {
+		PyErr_Format(DokiError, "[%s] Failed to allocate result matrix", tag);
+		return NULL;
+	}
+	switch (op) {
+	case '*':
+		m->s = src->s * z;
+		break;
+	case '/':
+		m->s = src->s / z;
+		break;
+	case 'T':
+		m->transpose = !src->transpose;
+		break;
+	default: /* 'H' */
+		m->transpose = !src->transpose;
+		m->conjugate = !src->conjugate;
+		break;
+	}
+	return wrap_fmat(m);
+}
+
+static int fm_scalar(PyObject *v, double complex *z)
+{
+	if (py_to_complex(v, z)) {
+		PyErr_SetString(DokiError, "scalar is not a number");
+		return -1;
+	}
+	return 0;
+}
+
+static PyObject *doki_funmatrix_scalar_mul(PyObject *self, PyObject *args)
+{
+	PyObject *cap, *raw;
+	int verbose;
+	double complex z;
+	if (!PyArg_ParseTuple(args, "OOp", &cap, &raw, &verbose)) {
+		PyErr_SetString(DokiError, "Syntax: funmatrix_mul(funmatrix, scalar, verbose)");
+		return NULL;
+	}
+	if (fm_scalar(raw, &z))
+		return NULL;
+	return fm_modified(cap, "SPROD", '*', z);
+}
+
+static PyObject *doki_funmatrix_scalar_div(PyObject *self, PyObject *args)
+{
+	PyObject *cap, *raw;
+	int verbose;
+	double complex z;
+	if (!PyArg_ParseTuple(args, "OOp", &cap, &raw, &verbose)) {
+		PyErr_SetString(DokiError, "Syntax: funmatrix_div(funmatrix, scalar, verbose)");
+		return NULL;
+	}
+	if (fm_scalar(raw, &z))
+		return NULL;
+	if (creal(z) == 0 && cimag(z) == 0) {
+		PyErr_SetString(DokiError, "Dividing by zero");
+		return NULL;
+	}
+	return fm_modified(cap, "SDIV", '/', z);
+}
+
+static PyObject *doki_funmatrix_transpose(PyObject *self, PyObject *args)
+{
+	PyObject *cap;
+	int verbose;
+	if (!PyArg_ParseTuple(args, "Op", &cap, &verbose)) {
+		PyErr_SetString(DokiError, "Syntax: funmatrix_transpose(funmatrix, verbose)");
+		return NULL;
+	}
+	return fm_modified(cap, "TRANS", 'T', 0.0);
+}
+
+static PyObject *doki_funmatrix_dagger(PyObject *self, PyObject *args)
+{
+	PyObject *cap;
+	int verbose;
+	if (!PyArg_ParseTuple(args, "Op", &cap, &verbose)) {
+		PyErr_SetString(DokiError, "Syntax: funmatrix_dagger(funmatrix, verbose)");
+		return NULL;
+	}
+	return fm_modified(cap, "HTRANS", 'H', 0.0);
+}
+
+static PyObject *doki_funmatrix_eyekron(PyObject *self, PyObject *args)
+{
+	PyObject *cap;
+	unsigned int left, right;
+	int verbose;
+	if (!PyArg_ParseTuple(args, "OIIp", &cap, &left, &right, &verbose)) {
+		PyErr_SetString(DokiError,
+				"Syntax: funmatrix_eyekron(funmatrix, leftQubits, rightQubits, verbose)");
+		return NULL;
+	}
+	fmat *u = get_fmat_msg(cap, "[EYEKRON] The matrix is NULL");
+	if (!u)
+		return NULL;
+	const int lr = ilog2(u->r > u->c ? u->r : u->c);
+	if ((uint64_t)left + right + (uint64_t)lr > 63) {
+		PyErr_SetString(DokiError, "[EYEKRON] Failed to allocate result matrix");
+		return NULL;
+	}
+	fmat *m = fmat_new(FM_EYEKRON, (1ull << left) * u->r * (1ull << right),
+			   (1ull << left) * u->c * (1ull << right));
+	if (!m) {
+		PyErr_SetString(DokiError, "[EYEKRON] Failed to allocate result matrix");
+		return NULL;
+	}
+	m->left = 1ull << left;
+	m->right = 1ull << right;
+	Py_INCREF(cap);
+	m->a = cap;
+	return wrap_fmat(m);
+}
+
+static PyObject *doki_funmatrix_projection(PyObject *self, PyObject *args)
+{
+	PyObject *cap;
+	unsigned int qubit;
+	int value, verbose;
+	if (!PyArg_ParseTuple(args, "OIpp", &cap, &qubit, &value, &verbose)) {
+		PyErr_SetString(DokiError,
+				"Syntax: funmatrix_projection(funmatrix, qubit_id, value, verbose)");
+		return NULL;
+	}
+	fmat *u = get_fmat_msg(cap, "[PROJ] The matrix is NULL");
+	if (!u)
+		return NULL;
+	if (qubit > 63) {
+		PyErr_SetString(DokiError, "[PROJ] Could not allocate data struct");
+		return NULL;
+	}
+	fmat *m = fmat_new(FM_PROJECTION, u->r, u->c);
+	if (!m) {
+		PyErr_SetString(DokiError, "[PROJ] Failed to allocate result matrix");
+		return NULL;
+	}
+	m->elem = (int)qubit;
+	m->value = value ? 1 : 0;
+	Py_INCREF(cap);
+	m->a = cap;
+	return wrap_fmat(m);
+}
+
+/* Qubit ids of a set for funmatrix_apply (doki.c:2331-2383); -1 on error. */
+static int fm_apply_ids(PyObject *set, unsigned nq, const char *type_msg, const char *range_msg,
+			uint64_t *mask)
+{
+	PyObject *it = PyObject_GetIter(set);
+	if (!it)
+		return -1;
+	PyObject *v;
+	while ((v = PyIter_Next(it))) {
+		if (!PyLong_Check(v)) {
+			Py_DECREF(v);
+			Py_DECREF(it);
+			PyErr_SetString(DokiError, type_msg);
+			return -1;
+		}
+		const long q = PyLong_AsLong(v);
+		Py_DECREF(v);
+		if (q < 0 || (unsigned long)q >= nq) {
+			Py_DECREF(it);
+			PyErr_Clear();
+			PyErr_SetString(DokiError, range_msg);
+			return -1;
+		}
+		*mask |= 1ull << q;
+	}
+	Py_DECREF(it);
+	return PyErr_Occurred() ? -1 : 0;
+}
+
+static PyObject *doki_funmatrix_apply(PyObject *self, PyObject *args)
+{
+	PyObject *scap, *gcap, *tlist, *cset, *aset;
+	int verbose;
+	if (!PyArg_ParseTuple(args, "OOOOOp", &scap, &gcap, &tlist, &cset, &aset, &verbose)) {
+		PyErr_SetString(DokiError, "Syntax: funmatrix_apply(registry, gate, target_list, "
+					   "control_set, anticontrol_set, verbose)");
+		return NULL;
+	}
+	fmat *st = get_fmat_msg(scap, "NULL pointer to registry");
+	if (!st)
+		return NULL;
+	fmat *g = get_fmat_msg(gcap, "NULL pointer to gate");
+	if (!g)
+		return NULL;
+	if (st->c > 1) {
+		PyErr_SetString(DokiError, "registry is not a column vector");
+		return NULL;
+	}
+	if (g->c != g->r) {
+		PyErr_SetString(DokiError, "gates have to be square matrices");
+		return NULL;
+	}
+	if (g->r > st->r) {
+		PyErr_SetString(DokiError, "gate is too big for this state vector");
+		return NULL;
+	}
+	const int nq = ilog2(st->r);
+	if (nq > 63 || st->r != (1ull << nq)) {
+		PyErr_SetString(DokiError, "registry needs 2^n rows");
+		return NULL;
+	}
+	const int ng = ilog2(g->r);
+	if (ng > 63 || g->r != (1ull << ng)) {
+		PyErr_SetString(DokiError, "gates need 2^n x 2^n elements");
+		return NULL;
+	}
+	if (!PyList_Check(tlist)) {
+		PyErr_SetString(DokiError, "target_list must be a list");
+		return NULL;
+	}
+	const Py_ssize_t nt = PyList_Size(tlist);
+	if (nt != ng) {
+		PyErr_SetString(DokiError, "Wrong number of targets specified for that gate");
+		return NULL;
+	}
+	const int have_c = PySet_Check(cset), have_a = PySet_Check(aset);
+	if (!have_c && cset != Py_None) {
+		PyErr_SetString(DokiError, "control_set must be a set or None");
+		return NULL;
+	}
+	if (!have_a && aset != Py_None) {
+		PyErr_SetString(DokiError, "anticontrol_set must be a set or None");
+		return NULL;
+	}
+	uint64_t cmask = 0, amask = 0;
+	if (have_c && PySet_Size(cset) > 0 &&
+	    fm_apply_ids(cset, (unsigned)nq,
+			 "control_set must be a set qubit ids (unsigned integers)",
+			 "Control qubit out of range", &cmask))
+		return NULL;
+	if (have_a && PySet_Size(aset) > 0) {
+		/* the reference tests each anticontrol for membership in the
+		 * control argument, which fails unless that argument is a set */
+		if (!have_c) {
+			PyErr_SetString(DokiError, "A control cannot also be an anticontrol");
+			return NULL;
+		}
+		PyObject *it = PyObject_GetIter(aset);
+		if (!it)
+			return NULL;
+		PyObject *v;
+		while ((v = PyIter_Next(it))) {
+			if (!PyLong_Check(v)) {
+				Py_DECREF(v);
+				Py_DECREF(it);
+				PyErr_SetString(DokiError, "anticontrol_set must be a set qubit ids "
+							   "(unsigned integers)");
+				return NULL;
+			}
+			const int clash = PySet_Contains(cset, v);
+			const long q = PyLong_AsLong(v);
+			Py_DECREF(v);
+			if (clash) {
+				Py_DECREF(it);
+				PyErr_Clear();
+				PyErr_SetString(DokiError, "A control cannot also be an anticontrol");
+				return NULL;
+			}
+			if (q < 0 || (unsigned long)q >= (unsigned long)nq) {
+				Py_DECREF(it);
+				PyErr_Clear();
+				PyErr_SetString(DokiError, "Anticontrol qubit out of range");
+				return NULL;
+			}
+			amask |= 1ull << q;
+		}
+		Py_DECREF(it);
+		if (PyErr_Occurred())
+			return NULL;
+	}
+	unsigned *targets = (unsigned *)malloc(sizeof(unsigned) * (nt ? (size_t)nt : 1));
+	if (!targets) {
+		PyErr_SetString(DokiError, "Failed to allocate target array");
+		return NULL;
+	}
+	for (Py_ssize_t k = 0; k < nt; k++) {
+		PyObject *v = PyList_GetItem(tlist, k);
+		if (!PyLong_Check(v)) {
+			free(targets);
+			PyErr_SetString(DokiError,
+					"target_list must be a list of qubit ids (unsigned integers)");
+			return NULL;
+		}
+		if ((have_c && PySet_Size(cset) > 0 && PySet_Contains(cset, v)) ||
+		    (have_a && PySet_Size(aset) > 0 && PySet_Contains(aset, v))) {
+			free(targets);
+			PyErr_SetString(DokiError,
+					"A target cannot also be a control or an anticontrol");
+			return NULL;
+		}
+		const long q = PyLong_AsLong(v);
+		if (q < 0 || q >= nq) {
+			free(targets);
+			PyErr_Clear();
+			PyErr_SetString(DokiError, "Target qubit out of range");
+			return NULL;
+		}
+		targets[k] = (unsigned)q;
+	}
+	fmat *m = fmat_new(FM_APPLY, st->r, 1);
+	if (!m) {
+		free(targets);
+		PyErr_SetString(DokiError, "[FMAPPLY] Failed to allocate matrix");
+		return NULL;
+	}
+	m->targets = targets;
+	m->ntargets = (unsigned)nt;
+	m->cmask = cmask;
+	m->amask = amask;
+	Py_INCREF(scap);
+	m->a = scap;
+	Py_INCREF(gcap);
+	m->b = gcap;
+	return wrap_fmat(m);
+}
 
 static PyMethodDef DokiMethods[] = {
 	{ "gate_new", doki_gate_new, METH_VARARGS, "Create new gate" },
@@ -1475,24 +2180,36 @@ static PyMethodDef DokiMethods[] = {
 	  "Same gate with a control qubit" },
 	{ "funmatrix_get", doki_funmatrix_get, METH_VARARGS,
 	  "Get a value from a functional matrix" },
-	{ "funmatrix_add", doki_funmatrix_add, METH_VARARGS, "Not supported" },
-	{ "funmatrix_sub", doki_funmatrix_sub, METH_VARARGS, "Not supported" },
-	{ "funmatrix_scalar_mul", doki_funmatrix_scalar_mul, METH_VARARGS, "Not supported" },
-	{ "funmatrix_scalar_div", doki_funmatrix_scalar_div, METH_VARARGS, "Not supported" },
-	{ "funmatrix_matmul", doki_funmatrix_matmul, METH_VARARGS, "Not supported" },
-	{ "funmatrix_ewmul", doki_funmatrix_ewmul, METH_VARARGS, "Not supported" },
-	{ "funmatrix_kron", doki_funmatrix_kron, METH_VARARGS, "Not supported" },
-	{ "funmatrix_eyekron", doki_funmatrix_eyekron, METH_VARARGS, "Not supported" },
-	{ "funmatrix_transpose", doki_funmatrix_transpose, METH_VARARGS, "Not supported" },
-	{ "funmatrix_dagger", doki_funmatrix_dagger, METH_VARARGS, "Not supported" },
-	{ "funmatrix_projection", doki_funmatrix_projection, METH_VARARGS, "Not supported" },
+	{ "funmatrix_add", doki_funmatrix_add, METH_VARARGS,
+	  "Addition of two functional matrices" },
+	{ "funmatrix_sub", doki_funmatrix_sub, METH_VARARGS,
+	  "Subtraction of two functional matrices" },
+	{ "funmatrix_scalar_mul", doki_funmatrix_scalar_mul, METH_VARARGS,
+	  "Product of a scalar and a functional matrix" },
+	{ "funmatrix_scalar_div", doki_funmatrix_scalar_div, METH_VARARGS,
+	  "Division of a functional matrix by a scalar" },
+	{ "funmatrix_matmul", doki_funmatrix_matmul, METH_VARARGS,
+	  "Matrix product of two functional matrices" },
+	{ "funmatrix_ewmul", doki_funmatrix_ewmul, METH_VARARGS,
+	  "Element-wise product of two functional matrices" },
+	{ "funmatrix_kron", doki_funmatrix_kron, METH_VARARGS,
+	  "Kronecker product of two functional matrices" },
+	{ "funmatrix_eyekron", doki_funmatrix_eyekron, METH_VARARGS,
+	  "I(2^left) (x) U (x) I(2^right)" },
+	{ "funmatrix_transpose", doki_funmatrix_transpose, METH_VARARGS,
+	  "Transpose of a functional matrix" },
+	{ "funmatrix_dagger", doki_funmatrix_dagger, METH_VARARGS,
+	  "Conjugate transpose of a functional matrix" },
+	{ "funmatrix_projection", doki_funmatrix_projection, METH_VARARGS,
+	  "Projection of a functional matrix on one value of a qubit" },
 	{ "funmatrix_shape", doki_funmatrix_shape, METH_VARARGS,
 	  "Get a tuple with the shape of the matrix" },
 	{ "funmatrix_partialtrace", doki_funmatrix_partialtrace, METH_VARARGS,
 	  "Get the partial trace of a functional matrix" },
 	{ "funmatrix_trace", doki_funmatrix_trace, METH_VARARGS,
 	  "Get the trace of a functional matrix" },
-	{ "funmatrix_apply", doki_funmatrix_apply, METH_VARARGS, "Not supported" },
+	{ "funmatrix_apply", doki_funmatrix_apply, METH_VARARGS,
+	  "Functional column vector after applying a gate to a functional state" },
 	{ "funmatrix_mem", doki_funmatrix_mem, METH_VARARGS,
 	  "Get the memory allocated by this FMatrix in bytes" },
 	{ "registry_get_all", doki_registry_get_all, METH_VARARGS,

@@ -333,6 +333,53 @@ def test_reduced_density_vs_oracle(dk_gpu, orc, oracle_mod):
     assert abs(d.funmatrix_trace(pt, False) - np.trace(want)) < 1e-11
 
 
+def test_density_algebra_vs_oracle(dk_gpu, orc, oracle_mod):
+    """Lazy algebra over register-backed density matrices: modifiers on top of
+    the device reduced-density path, modified nodes inside a partial-trace
+    chain (element-wise path), products and a gate applied to a column."""
+    d = dk_gpu
+    n = 6
+    ops = random_ops(W.rng_for(43), n, 40)
+    a = W.run_ops(d, d.registry_new(n, False), ops)
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    psi = orc.registry_get_all(b)
+    full = np.outer(psi, psi.conj())
+    rho = d.registry_density(a, False)
+    tol = dict(atol=ATOL_C128, rtol=0)
+    assert np.allclose(d.funmatrix_numpy(d.funmatrix_dagger(rho, False)), full.conj().T, **tol)
+    # device path under a scalar and a transpose on the top node
+    low5 = oracle_mod.reduced_density(b, 0b011111)
+    pt = d.funmatrix_partialtrace(rho, n - 1, False)
+    assert np.allclose(d.funmatrix_numpy(d.funmatrix_scalar_mul(pt, 2 - 1j, False)),
+                       (2 - 1j) * low5, **tol)
+    pt4 = d.funmatrix_partialtrace(pt, n - 2, False)
+    low4 = oracle_mod.reduced_density(b, 0b001111)
+    assert np.allclose(d.funmatrix_numpy(d.funmatrix_transpose(pt4, False)), low4.T, **tol)
+    # a modified node inside the chain: element-wise partial trace
+    scaled = d.funmatrix_scalar_div(rho, 4, False)
+    ptg = d.funmatrix_partialtrace(d.funmatrix_partialtrace(scaled, 0, False), 2, False)
+    keep = oracle_mod.kept_mask_after_traces(n, [0, 2])
+    assert np.allclose(d.funmatrix_numpy(ptg), oracle_mod.reduced_density(b, keep) / 4, **tol)
+    # products of reduced density matrices and identities
+    sq = d.funmatrix_matmul(pt4, pt4, False)
+    assert np.allclose(d.funmatrix_numpy(sq), low4 @ low4, **tol)
+    assert abs(d.funmatrix_trace(sq, False) - np.trace(low4 @ low4)) < 1e-12
+    kr = d.funmatrix_kron(pt4, d.funmatrix_identity(1, False), False)
+    assert np.allclose(d.funmatrix_numpy(kr), np.kron(low4, np.eye(2)), **tol)
+    ek = d.funmatrix_eyekron(pt4, 1, 0, False)
+    assert np.allclose(d.funmatrix_numpy(ek), np.kron(np.eye(2), low4), **tol)
+    # a Hadamard on qubit 3 of column 0 of rho (psi * conj(psi_0))
+    col = d.funmatrix_matmul(rho, d.funmatrix_statezero(n, False), False)
+    h = d.funmatrix_apply(col, d.funmatrix_hadamard(1, False), [3], {1}, None, False)
+    x = full[:, 0]
+    want = x.copy()
+    for i in range(1 << n):
+        if i & 2:
+            lo, hi = x[i & ~8], x[i | 8]
+            want[i] = (lo + hi) / np.sqrt(2) if not i & 8 else (lo - hi) / np.sqrt(2)
+    assert np.allclose(d.funmatrix_numpy(h)[:, 0], want, **tol)
+
+
 @pytest.mark.parametrize("n,keep_bits,prec", [(12, 3, 2), (16, 5, 2), (16, 6, 2), (18, 8, 2),
                                                (20, 10, 2), (18, 7, 1), (17, 9, 2)])
 def test_reduced_density_sizes(dk_gpu, orc, oracle_mod, n, keep_bits, prec):

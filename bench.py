@@ -61,7 +61,9 @@ def workload_config(n, depth, c):
                      "reduced density matrix of qubits 0-9"),
         "qubits": n, "depth": depth, "gates": len(c.ops),
         "state_bytes": 16 << n,
-        "l2": "inputs larger than L2 (state 16 GiB vs 126 MB L2)",
+        "l2": (f"inputs larger than L2 (state {(16 << n) / 2**30:g} GiB vs 126 MB L2)"
+               if (16 << n) > 126e6 else
+               f"state {(16 << n) / 2**20:g} MiB fits in the 126 MB L2 (not flushed)"),
         "parallelism": "replicas",
     }
 

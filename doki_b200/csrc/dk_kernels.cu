@@ -1815,6 +1815,38 @@ cudaError_t launch_herm_fill(const double2 *C, double2 *rho, uint64_t dim,
 	return cudaGetLastError();
 }
 
+/* Dynamic shared memory of k_rho_tc: two slab buffers of the row and column
+ * tiles.  The attribute is set once; the occupancy it allows is cached. */
+constexpr size_t kRhoSmem = sizeof(double2) * 2 * 2 * kRhoSlab * kRhoTile;
+
+static cudaError_t rho_prepare(int *ctas_per_sm)
+{
+	static std::once_flag once;
+	static cudaError_t err = cudaSuccess;
+	static int occ = 1;
+	std::call_once(once, [&] {
+		err = cudaFuncSetAttribute(k_rho_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+					   (int)kRhoSmem);
+		int o = 0;
+		if (err == cudaSuccess &&
+		    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_rho_tc, 256, kRhoSmem) ==
+			    cudaSuccess &&
+		    o > 0)
+			occ = o;
+		cudaGetLastError();
+	});
+	if (ctas_per_sm)
+		*ctas_per_sm = occ;
+	return err;
+}
+
+/* Traced-range splits of the reduced density product.  Tiles x splits CTAs
+ * should fill whole waves of the resident CTA slots (a 1024 x 1024 result
+ * has 136 tiles; 13 splits fill 12 waves of 148 at 99.5 %, where 8 would
+ * leave the last of 8 waves a third full); each split keeps at least 256
+ * traced values, there are at most 64 and their partials stay within 1 GiB.
+ * Among split counts giving at least two waves, a larger count is taken only
+ * when it fills the waves 2 % better. */
 int rho_splits(uint64_t dim, uint64_t K, int num_sms)
 {
 	if (dim < (uint64_t)kRhoTile) {
@@ -1824,10 +1856,25 @@ int rho_splits(uint64_t dim, uint64_t K, int num_sms)
 		return ns ? (int)ns : 1;
 	}
 	const uint64_t T = dim / kRhoTile, ntile = T * (T + 1) / 2;
-	uint64_t ns = 1;
-	while (ntile * ns < (uint64_t)num_sms * 4 && ns * 256 <= K && ns < 64)
-		ns *= 2;
-	return (int)ns;
+	int occ = 1;
+	rho_prepare(&occ);
+	const uint64_t slots = (uint64_t)(num_sms > 0 ? num_sms : 1) * (uint64_t)occ;
+	const uint64_t part_cap = (1ull << 30) / (16 * dim * dim);
+	uint64_t best = 1;
+	double best_fill = -1.0;
+	for (uint64_t ns = 1; ns <= 64 && ns * 256 <= K && (ns == 1 || ns <= part_cap); ++ns) {
+		const uint64_t ctas = ntile * ns;
+		const bool more_allowed = ns < 64 && (ns + 1) * 256 <= K && ns + 1 <= part_cap;
+		if (ctas < 2 * slots && more_allowed)
+			continue;
+		const uint64_t waves = (ctas + slots - 1) / slots;
+		const double fill = (double)ctas / (double)(waves * slots);
+		if (fill > best_fill + 0.02) {
+			best = ns;
+			best_fill = fill;
+		}
+	}
+	return (int)best;
 }
 
 cudaError_t launch_rho(const double2 *A, uint64_t dim, uint64_t K, double alpha, int nsplit,
@@ -1844,17 +1891,11 @@ cudaError_t launch_rho(const double2 *A, uint64_t dim, uint64_t K, double alpha,
 	const uint64_t T = dim / kRhoTile, ntile = T * (T + 1) / 2;
 	uint64_t bchunk = (K + nsplit - 1) / nsplit;
 	bchunk = (bchunk + kRhoSlab - 1) / kRhoSlab * kRhoSlab;
-	const size_t smem = sizeof(double2) * 2 * 2 * kRhoSlab * kRhoTile;
-	static std::once_flag once;
-	static cudaError_t set_err = cudaSuccess;
-	std::call_once(once, [&] {
-		set_err = cudaFuncSetAttribute(k_rho_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-					       (int)smem);
-	});
+	const cudaError_t set_err = rho_prepare(nullptr);
 	if (set_err != cudaSuccess)
 		return set_err;
 	dim3 grid((unsigned)ntile, (unsigned)nsplit);
-	k_rho_tc<<<grid, 256, smem, st>>>(A, dim, K, bchunk, nsplit == 1 ? C : part, alpha);
+	k_rho_tc<<<grid, 256, kRhoSmem, st>>>(A, dim, K, bchunk, nsplit == 1 ? C : part, alpha);
 	g_launches += 1;
 	if (nsplit > 1) {
 		const int blocks = grid_for(dim * dim, 256 * 4, g_num_sms * 8);

@@ -310,6 +310,101 @@ __device__ __forceinline__ void tc_product(const double2 &e0, const double2 &e1,
 	y[3] = p3[1] - p1[1] - p2[1];
 }
 
+/* TF32 tensor-core MMA, D (16x8, f32) += A (16x8, row-major) * B (8x8,
+ * column-major).  Lane l = 4 g + t holds A[g][t], A[g+8][t], A[g][t+4],
+ * A[g+8][t+4], B[t][g], B[t+4][g] and D[g][2t], D[g][2t+1], D[g+8][2t],
+ * D[g+8][2t+1]: the B and D lane layouts of the FP64 m8n8k4 MMA above. */
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+					 uint32_t b1)
+{
+	asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, "
+	    "{%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+	    : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+	    : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+/* x = hi + lo exactly, hi = x with its 13 low mantissa bits cleared (a TF32
+ * value).  The MMA reads lo as TF32 too (its low 13 bits ignored), so hi + lo
+ * reaches the product with about 21 bits of x. */
+__device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo)
+{
+	hi = __float_as_uint(x) & 0xffffe000u;
+	lo = __float_as_uint(x - __uint_as_float(hi));
+}
+
+/* Lane fragments of one 8x8 matrix entry and the column-group product y = M x
+ * of a tensor sweep, per amplitude precision.  complex128: FP64 MMAs in the
+ * Gauss form (tc_product).  complex64: the real form
+ *   [yr; yi] = [[Mr, -Mi], [Mi, Mr]] [xr; xi]
+ * as one 16x16-by-16x8 product, i.e. two k-steps of the TF32 m16n8k8 MMA
+ * (k-step 0 multiplies xr by [Mr; Mi], k-step 1 xi by [-Mi; Mr]).  Operands
+ * are split into TF32 hi + lo parts and each k-step takes hi*hi + hi*lo +
+ * lo*hi (the lo*lo term is below FP32 rounding), accumulated in FP32, so the
+ * product carries close to FP32 precision.  Lane l = 4 g + t reads matrix entries
+ * (g, t) and (g, t + 4) in both precisions. */
+template <typename R> struct TcFrag;
+
+template <> struct TcFrag<double> {
+	double2 e0, e1;
+	__device__ __forceinline__ void load(const double2 *mt)
+	{
+		e0 = __ldg(mt);
+		e1 = __ldg(mt + 4);
+	}
+	__device__ __forceinline__ void product(const double2 &x0, const double2 &x1,
+						double (&y)[4]) const
+	{
+		tc_product(e0, e1, x0, x1, y);
+	}
+};
+
+template <> struct TcFrag<float> {
+	uint32_t k0h[4], k0l[4], k1h[4], k1l[4];
+	__device__ __forceinline__ void load(const double2 *mt)
+	{
+		const double2 e0 = __ldg(mt), e1 = __ldg(mt + 4);
+		const float a0[4] = { (float)e0.x, (float)e0.y, (float)e1.x, (float)e1.y };
+		const float a1[4] = { -(float)e0.y, (float)e0.x, -(float)e1.y, (float)e1.x };
+#pragma unroll
+		for (int i = 0; i < 4; ++i) {
+			tf32_split(a0[i], k0h[i], k0l[i]);
+			tf32_split(a1[i], k1h[i], k1l[i]);
+		}
+	}
+	__device__ __forceinline__ void product(const float2 &x0, const float2 &x1,
+						float (&y)[4]) const
+	{
+		uint32_t r0h, r0l, r1h, r1l, i0h, i0l, i1h, i1l;
+		tf32_split(x0.x, r0h, r0l);
+		tf32_split(x1.x, r1h, r1l);
+		tf32_split(x0.y, i0h, i0l);
+		tf32_split(x1.y, i1h, i1l);
+		/* the two k-steps accumulate separately (two dependency chains),
+		 * small terms first */
+		float u[4] = { 0.0f, 0.0f, 0.0f, 0.0f };
+		y[0] = y[1] = y[2] = y[3] = 0.0f;
+		mma_tf32(y, k0l, r0h, r1h);
+		mma_tf32(u, k1l, i0h, i1h);
+		mma_tf32(y, k0h, r0l, r1l);
+		mma_tf32(u, k1h, i0l, i1l);
+		mma_tf32(y, k0h, r0h, r1h);
+		mma_tf32(u, k1h, i0h, i1h);
+#pragma unroll
+		for (int i = 0; i < 4; ++i)
+			y[i] += u[i];
+	}
+};
+
+template <typename C2, typename R> __device__ __forceinline__ C2 c2_make(R re, R im);
+template <> __device__ __forceinline__ double2 c2_make<double2, double>(double re, double im)
+{
+	return make_double2(re, im);
+}
+template <> __device__ __forceinline__ float2 c2_make<float2, float>(float re, float im)
+{
+	return make_float2(re, im);
+}
+
 template <typename R, int SW, int M, int MINB>
 __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 	k_sweep_tc(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
@@ -467,26 +562,29 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 				const double2 *mb = mats + 64 * (size_t)tc_matrix(sg[__ldg(&pn->g0)],
 										  scond, base) +
 						    8 * gl + gk;
-				const double2 e0 = __ldg(ma), e1 = __ldg(ma + 4);
+				/* the second entry's fragments are reloaded per group (L1),
+				 * which keeps three CTAs per SM */
+				TcFrag<R> fa, fb;
+				fa.load(ma);
 #pragma unroll
 				for (int hq = 0; hq < 4 * VT; ++hq) {
 					const int q = hq & 3, h = hq >> 2;
 					const uint32_t sgl = sgl0 ^ __ldg(&pd->shi[warp + 8u * h]);
 					const uint32_t sgk = sgk0 ^ __ldg(&pn->shi[warp + 8u * h]);
 					const uint32_t bg = sgl ^ ((q & 1) ? t8 : 0u) ^ ((q & 2) ? t16 : 0u);
-					const double2 x0 = to_c128(tile[bg ^ gj0]);
-					const double2 x1 = to_c128(tile[bg ^ gj1]);
-					double y[4], z[4];
-					tc_product(e0, e1, x0, x1, y);
+					const C2 x0 = tile[bg ^ gj0];
+					const C2 x1 = tile[bg ^ gj1];
+					R y[4], z[4];
+					fa.product(x0, x1, y);
+					fb.load(mb);
 					/* amplitude l%4 and 4 + l%4 of column l/4 in the next pass */
-					tc_product(__ldg(mb), __ldg(mb + 4), make_double2(y[0], y[2]),
-						   make_double2(y[1], y[3]), z);
+					fb.product(c2_make<C2, R>(y[0], y[2]), c2_make<C2, R>(y[1], y[3]), z);
 					__syncwarp(); /* the group's gathers precede its writes */
 #pragma unroll
 					for (int e = 0; e < 2; ++e) {
 						const uint32_t bs = sgk ^ (e ? u1 : 0u) ^ ((q & 1) ? u8 : 0u) ^
 								    ((q & 2) ? u16 : 0u);
-						tile[bs ^ sr] = from_c128<C2>(make_double2(z[e], z[2 + e]));
+						tile[bs ^ sr] = c2_make<C2, R>(z[e], z[2 + e]);
 					}
 				}
 				__syncwarp();
@@ -518,7 +616,8 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 				}
 				/* lane fragments: entries (l/4, l%4) and (l/4, 4 + l%4) */
 				const double2 *mt = mats + 64 * (size_t)tc_matrix(d, scond, base) + 8 * gl + gk;
-				const double2 e0 = __ldg(mt), e1 = __ldg(mt + 4);
+				TcFrag<R> fa;
+				fa.load(mt);
 				const bool ctl = (d.x & 0xffffu) == DK_GC_DENSE3 + 1;
 				/* one column group at a time: the groups' slots are
 				 * disjoint */
@@ -528,10 +627,10 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 					const uint32_t shw = __ldg(&pd->shi[warp + 8u * h]);
 					const uint32_t sgl = sgl0 ^ shw, sgk = sgk0 ^ shw;
 					const uint32_t bg = sgl ^ ((q & 1) ? t8 : 0u) ^ ((q & 2) ? t16 : 0u);
-					const double2 x0 = to_c128(tile[bg ^ gj0]);
-					const double2 x1 = to_c128(tile[bg ^ gj1]);
-					double y[4];
-					tc_product(e0, e1, x0, x1, y);
+					const C2 x0 = tile[bg ^ gj0];
+					const C2 x1 = tile[bg ^ gj1];
+					R y[4];
+					fa.product(x0, x1, y);
 					__syncwarp(); /* the group's gathers precede its writes */
 #pragma unroll
 					for (int e = 0; e < 2; ++e) {
@@ -544,7 +643,7 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 						}
 						const uint32_t bs = sgk ^ (e ? t1 : 0u) ^ ((q & 1) ? t8 : 0u) ^
 								    ((q & 2) ? t16 : 0u);
-						tile[bs ^ sr] = from_c128<C2>(make_double2(y[e], y[2 + e]));
+						tile[bs ^ sr] = c2_make<C2, R>(y[e], y[2 + e]);
 					}
 				}
 				__syncwarp();
@@ -1113,7 +1212,7 @@ __global__ void __launch_bounds__(256)
  * products go to part[s] and are added in a fixed order by k_rho_reduce. */
 
 constexpr int kRhoTile = 64; /* output tile (rows and columns) */
-constexpr int kRhoSlab = 16; /* traced values per shared-memory slab */
+constexpr int kRhoSlab = 32; /* traced values per shared-memory slab */
 
 __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, bool valid)
 {
@@ -1126,8 +1225,9 @@ __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, b
  * 8 warps as 2 x 4: a warp owns rows 32 wr .. +32 (4 MMA row blocks) and
  * columns 16 wc .. +16 (2 column blocks).  Per 4 traced values (one k-step)
  * each 8x8 block takes 3 FP64 MMAs (Gauss): P1 += Xr Xr'^T, P2 += Xi Xi'^T,
- * P3 += (Xr + Xi)(Xr' - Xi')^T; re = P1 + P2, im = P3 - P1 + P2.  The 24
- * accumulators of a lane need one CTA per SM. 
+ * P3 += (Xr + Xi)(Xr' - Xi')^T; re = P1 + P2, im = P3 - P1 + P2.  The 48
+ * accumulators of a lane need one CTA per SM; slabs of 32 traced values
+ * (128 KiB double-buffered) keep block barriers to one per 8 k-steps.
  * Slabs are stored [b][a ^ 2 (b & 3)] so a quarter-warp's fragment reads
  * (4 traced rows x 2 columns) hit 8 distinct 16-byte bank groups. */
 __global__ void __launch_bounds__(256, 1)
@@ -1501,7 +1601,8 @@ cudaError_t launch_sweep(int prec, const void *in, void *out,
 	int blocks = 0;
 	cudaError_t e;
 	if (hp->mode == DK_SWEEP_TENSOR) {
-		/* FP64 tensor-core passes; tiles of 8 to 12 bits */
+		/* tensor-core passes (FP64 for complex128, split TF32 for
+		 * complex64); tiles of 8 to 12 bits */
 		if (prec == DK_C128)
 			e = m >= 12 ? run_sweep_tc<double, 3, 12, DK_TC_MINB12>(in, out, dprog, hp,
 										num_sms, s, st, &blocks)

@@ -50,20 +50,25 @@ def parse():
     p.add_argument("--no-forms", action="store_true",
                    help="skip the batching / serving / precision forms")
     p.add_argument("--serve-requests", type=int, default=120)
+    p.add_argument("--precision", choices=("c128", "c64"), default="c128",
+                   help="register precision of the plain workload (c64: split-TF32 "
+                        "tensor products, FP64 norms)")
     return p.parse_args()
 
 
-def workload_config(n, depth, c):
+def workload_config(n, depth, c, prec="c128"):
+    amp = 16 if prec == "c128" else 8
     return {
-        "workload": (f"{n}-qubit complex128 register, seeded depth-{depth} random circuit "
+        "workload": (f"{n}-qubit {'complex128' if prec == 'c128' else 'complex64'} register, "
+                     f"seeded depth-{depth} random circuit "
                      "(U3 on all qubits + CZ/CNOT brickwork, 5% gates with 1-3 extra "
                      "controls/anticontrols), all marginals, measure+collapse of 4 qubits, "
                      "reduced density matrix of qubits 0-9"),
         "qubits": n, "depth": depth, "gates": len(c.ops),
-        "state_bytes": 16 << n,
-        "l2": (f"inputs larger than L2 (state {(16 << n) / 2**30:g} GiB vs 126 MB L2)"
-               if (16 << n) > 126e6 else
-               f"state {(16 << n) / 2**20:g} MiB fits in the 126 MB L2 (not flushed)"),
+        "state_bytes": amp << n,
+        "l2": (f"inputs larger than L2 (state {(amp << n) / 2**30:g} GiB vs 126 MB L2)"
+               if (amp << n) > 126e6 else
+               f"state {(amp << n) / 2**20:g} MiB fits in the 126 MB L2 (not flushed)"),
         "parallelism": "replicas",
     }
 
@@ -159,10 +164,10 @@ def job_rate(world, units_per_rank, seconds):
     return world * units_per_rank / seconds
 
 
-def run_job(d, c, gates, keep, rolls_mask, rolls):
+def run_job(d, c, gates, keep, rolls_mask, rolls, prec="c128"):
     """One full workload through the public API; returns the host results."""
     n = c.num_qubits
-    reg = d.registry_new(n, False)
+    reg = d.registry_new(n, False) if prec == "c128" else d.registry_new(n, False, 1)
     for op, g in zip(c.ops, gates):
         ctl = set(op.controls) if (op.controls or op.anticontrols) else None
         reg = d.registry_apply(reg, g, list(op.targets), ctl, set(op.anticontrols) or None,
@@ -205,7 +210,7 @@ def engine_arm(args, rank, world, local_rank):
 
     # warm-up (also creates the engine stream)
     for _ in range(args.warmup):
-        reg = run_job(d, c, gates, keep, mask, rolls)
+        reg = run_job(d, c, gates, keep, mask, rolls, args.precision)
         finish_job(d, reg, n, keep, mask, rolls)
         del reg
     d.engine_sync()
@@ -223,7 +228,7 @@ def engine_arm(args, rank, world, local_rank):
     st0 = d.engine_stats()
     dev_ms, sweep_ms, nsweeps = 0.0, 0.0, 0
     for _ in range(args.steps):
-        reg = run_job(d, c, gates, keep, mask, rolls)
+        reg = run_job(d, c, gates, keep, mask, rolls, args.precision)
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         e0.record(stream)
         s_before = d.engine_stats()["sweeps"]
@@ -248,7 +253,7 @@ def engine_arm(args, rank, world, local_rank):
     for _ in range(args.steps):
         t0 = time.perf_counter()
         g2 = [d.gate_new(op.k, op.gate.tolist(), False) for op in c.ops]
-        reg = run_job(d, c, g2, keep, mask, rolls)
+        reg = run_job(d, c, g2, keep, mask, rolls, args.precision)
         probs, res, mat = finish_job(d, reg, n, keep, mask, rolls)
         e2e_s += time.perf_counter() - t0
         del reg, g2
@@ -260,23 +265,26 @@ def engine_arm(args, rank, world, local_rank):
     layers = depth * args.steps
     value = job_rate(world, layers, dev_ms / 1e3)
     e2e_value = job_rate(world, layers, e2e_s)
-    state_bytes = 16 << n
+    c64 = args.precision == "c64"
+    state_bytes = (8 if c64 else 16) << n
     avg_sweep_s = (sweep_ms / 1e3) / max(1, nsweeps)
     achieved = 2 * state_bytes / avg_sweep_s / 1e9
     peak, peak_kind = measured_peak_hbm()
     tr = committed_traffic()
     traffic = None
-    if tr and tr.get("qubits"):
+    if tr and tr.get("qubits") and not c64:
         traffic = float(tr["bytes_per_launch"]) * (state_bytes / (16 << int(tr["qubits"])))
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(n, depth, c),
+        "vs_baseline": None, "dtype": "f32" if c64 else "f64", "data": "synthetic",
+        "config": workload_config(n, depth, c, args.precision),
         "roofline": {"bound": "hbm",
-                     "kernel": "k_sweep_tc<double> (fused gate sweep, FP64 tensor-core passes)",
+                     "kernel": ("k_sweep_tc<float> (fused gate sweep, split-TF32 tensor-core "
+                                "passes)" if c64 else
+                                "k_sweep_tc<double> (fused gate sweep, FP64 tensor-core passes)"),
                      "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind + " hbm_gbs (copy)", "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,

@@ -827,11 +827,32 @@ __global__ void k_clear_flags(dk_scal *sc)
 
 /* ---- marginals: S_q = sum_{bit q of i set} |amp_i|^2 for all q --------
  * Thread g visits i = (k << s) | g, s = log2(total threads): bits below s are
- * fixed per thread, bits above vary with k and are accumulated per bit. */
+ * fixed per thread, bits above vary with k and are accumulated per bit in
+ * acc[NB] (NB >= n - s, indexed only by unrolled constants so that it stays
+ * in registers).  Two 256-thread blocks fit per SM. */
 constexpr int kMargHi = 24;
 
-template <typename R>
-__global__ void __launch_bounds__(256)
+/* Block sum of v into partials[slot] (thread 0), uniform call sites only. */
+__device__ __forceinline__ void marg_store(double v, double *red, double *dst)
+{
+	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		v += __shfl_xor_sync(0xffffffffu, v, o);
+	if (l == 0)
+		red[w] = v;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int i = 0; i < (int)(blockDim.x >> 5); ++i)
+			t += red[i];
+		*dst = t;
+	}
+	__syncthreads();
+}
+
+template <typename R, int NB>
+__global__ void __launch_bounds__(256, 2)
 	k_marginals(const typename CT<R>::T *__restrict__ d, int n, int s,
 		    double *partials)
 {
@@ -840,10 +861,10 @@ __global__ void __launch_bounds__(256)
 	/* registers smaller than one warp: lanes past the register stay idle */
 	const uint64_t cnt = (g >> s) ? 0ull : (1ull << nb);
 	double tot = 0.0;
-	double hi[kMargHi];
+	double acc[NB];
 #pragma unroll
-	for (int j = 0; j < kMargHi; ++j)
-		hi[j] = 0.0;
+	for (int j = 0; j < NB; ++j)
+		acc[j] = 0.0;
 	if (cnt >= 16) {
 		/* 16 consecutive k at a time: the 4 low bits of k take fixed
 		 * patterns, every higher bit is constant over the group */
@@ -863,12 +884,12 @@ __global__ void __launch_bounds__(256)
 				for (int e = 0; e < 16; ++e)
 					if ((e >> j) & 1)
 						h += p[e];
-				hi[j] += h;
+				acc[j] += h;
 			}
 #pragma unroll
-			for (int j = 4; j < kMargHi; ++j)
+			for (int j = 4; j < NB; ++j)
 				if (j < nb && ((k0 >> j) & 1u))
-					hi[j] += t;
+					acc[j] += t;
 			tot += t;
 		}
 	} else {
@@ -876,42 +897,21 @@ __global__ void __launch_bounds__(256)
 			const double p = sqabs(__ldcs(d + ((k << s) | g)));
 			tot += p;
 #pragma unroll
-			for (int j = 0; j < kMargHi; ++j)
+			for (int j = 0; j < NB; ++j)
 				if (j < nb && ((k >> j) & 1u))
-					hi[j] += p;
+					acc[j] += p;
 		}
 	}
 	__shared__ double red[32];
-	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-	const int nw = blockDim.x >> 5;
-	/* values to reduce: q < s -> tot * bit_q(g); q = s + j -> hi[j]; q = n -> tot */
-	for (int q = 0; q <= n; ++q) {
-		double v;
-		if (q == n)
-			v = tot;
-		else if (q < s)
-			v = ((g >> q) & 1u) ? tot : 0.0;
-		else {
-			v = 0.0;
+	double *const out = partials + (size_t)blockIdx.x * kPartialStride;
+	/* q < s: tot * bit_q(g); q = s + j: acc[j]; q = n: tot */
+	for (int q = 0; q < s && q < n; ++q)
+		marg_store(((g >> q) & 1u) ? tot : 0.0, red, out + q);
 #pragma unroll
-			for (int j = 0; j < kMargHi; ++j)
-				if (j == q - s)
-					v = hi[j];
-		}
-#pragma unroll
-		for (int o = 16; o > 0; o >>= 1)
-			v += __shfl_xor_sync(0xffffffffu, v, o);
-		if (l == 0)
-			red[w] = v;
-		__syncthreads();
-		if (threadIdx.x == 0) {
-			double t = 0.0;
-			for (int i = 0; i < nw; ++i)
-				t += red[i];
-			partials[(size_t)blockIdx.x * kPartialStride + q] = t;
-		}
-		__syncthreads();
-	}
+	for (int j = 0; j < NB; ++j)
+		if (j < nb)
+			marg_store(acc[j], red, out + s + j);
+	marg_store(tot, red, out + n);
 }
 
 __global__ void k_marg_finalize(const double *partials, int nb, int n, double *marg)
@@ -1696,16 +1696,41 @@ cudaError_t launch_import(int prec, const double *src, void *d, unsigned n,
 	return cudaGetLastError();
 }
 
+/* k_marginals with the smallest accumulator array that holds the n - sbits
+ * bits each thread varies over. */
+static void launch_marginals_kernel(int prec, const void *d, unsigned n, int sbits, int blocks,
+				    int threads, double *partials, cudaStream_t st)
+{
+	const int nb = (int)n - sbits;
+#define DK_MARG(NB)                                                                      \
+	do {                                                                             \
+		if (prec == DK_C128)                                                     \
+			k_marginals<double, NB><<<blocks, threads, 0, st>>>(             \
+				(const double2 *)d, (int)n, sbits, partials);            \
+		else                                                                     \
+			k_marginals<float, NB><<<blocks, threads, 0, st>>>(              \
+				(const float2 *)d, (int)n, sbits, partials);             \
+	} while (0)
+	if (nb <= 12)
+		DK_MARG(12);
+	else if (nb <= 16)
+		DK_MARG(16);
+	else
+		DK_MARG(kMargHi);
+#undef DK_MARG
+}
+
 cudaError_t launch_marginals(int prec, const void *d, unsigned n, const Scratch &s,
 			     cudaStream_t st)
 {
+	/* up to 2048 blocks: 2 per SM make 6.9 waves of 296 at 30 qubits */
 	int threads = 256, blocks = 1;
 	if (n < 8)
 		threads = 1 << n;
 	else {
 		int lb = (int)n - 8;
-		if (lb > 10)
-			lb = 10;
+		if (lb > 11)
+			lb = 11;
 		blocks = 1 << lb;
 	}
 	int sbits = 0;
@@ -1718,12 +1743,7 @@ cudaError_t launch_marginals(int prec, const void *d, unsigned n, const Scratch 
 		threads = 32;
 		sbits = (int)n;
 	}
-	if (prec == DK_C128)
-		k_marginals<double><<<blocks, threads, 0, st>>>((const double2 *)d,
-							       (int)n, sbits, s.partials);
-	else
-		k_marginals<float><<<blocks, threads, 0, st>>>((const float2 *)d,
-							      (int)n, sbits, s.partials);
+	launch_marginals_kernel(prec, d, n, sbits, blocks, threads, s.partials, st);
 	k_marg_finalize<<<1, 64, 0, st>>>(s.partials, blocks, (int)n, s.marg);
 	g_launches += 2;
 	return cudaGetLastError();
@@ -1750,12 +1770,7 @@ cudaError_t launch_marginals_blocks(int prec, const void *d, unsigned n,
 		threads = 32;
 		sbits = (int)n;
 	}
-	if (prec == DK_C128)
-		k_marginals<double><<<blocks, threads, 0, st>>>((const double2 *)d,
-							       (int)n, sbits, s.partials);
-	else
-		k_marginals<float><<<blocks, threads, 0, st>>>((const float2 *)d,
-							      (int)n, sbits, s.partials);
+	launch_marginals_kernel(prec, d, n, sbits, blocks, threads, s.partials, st);
 	k_marg_finalize<<<1, 64, 0, st>>>(s.partials, blocks, (int)n, s.marg);
 	g_launches += 2;
 	return cudaGetLastError();

@@ -332,3 +332,30 @@ def test_element_errors_match_reference(dk, ref, rng, expr):
     # the NaN leaf itself
     assert _err(lambda: dk.funmatrix_get(nan[0], 0, 0, False)) == \
         _err(lambda: ref.funmatrix_get(nan[1], 0, 0, False))
+
+
+def test_nodes_release_their_operands(dk):
+    """Every node holds references to its operands only while it lives."""
+    import gc
+    import sys
+    A = dk.funmatrix_create([[1, 2], [3, 4]], False)
+    B = dk.funmatrix_identity(1, False)
+    col = dk.funmatrix_statezero(1, False)
+    base = [sys.getrefcount(o) for o in (A, B, col)]
+    for _ in range(50):
+        x = dk.funmatrix_add(A, B, False)
+        y = dk.funmatrix_dagger(x, False)
+        z = dk.funmatrix_scalar_mul(y, 2j, False)
+        k = dk.funmatrix_kron(z, A, False)
+        e = dk.funmatrix_eyekron(A, 1, 1, False)
+        p = dk.funmatrix_projection(k, 1, True, False)
+        ap = dk.funmatrix_apply(col, A, [0], None, None, False)
+        t = dk.funmatrix_partialtrace(k, 0, False)
+        with pytest.raises(dk.error):
+            dk.funmatrix_apply(col, A, [0], {5}, None, False)
+        dk.funmatrix_get(p, 1, 1, False)
+        dk.funmatrix_trace(t, False)
+        dk.funmatrix_numpy(ap)
+        del x, y, z, k, e, p, ap, t
+    gc.collect()
+    assert [sys.getrefcount(o) for o in (A, B, col)] == base

@@ -1138,6 +1138,39 @@ __global__ void __launch_bounds__(256)
 	}
 }
 
+/* Join with a least register larger than the L2 and a small most register:
+ * one thread per least amplitude, read once, times every most amplitude
+ * (k_join above re-reads the whole least register once per most amplitude).
+ * Same products as k_join; writes are coalesced over consecutive l. */
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_join_wide(const typename CT<R>::T *__restrict__ most, const dk_scal *sc1,
+		    const typename CT<R>::T *__restrict__ least, const dk_scal *sc2, int n1,
+		    int n2, typename CT<R>::T *out, double *partials)
+{
+	typedef typename CT<R>::T C2;
+	const double i1 = 1.0 / sc1->norm, i2 = 1.0 / sc2->norm;
+	const uint64_t nl = 1ull << n2, nm = 1ull << n1;
+	double s = 0.0, dummy = 0.0;
+	for (uint64_t l = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; l < nl;
+	     l += (uint64_t)gridDim.x * blockDim.x) {
+		const double2 b = to_c128(__ldcs(least + l));
+		const double2 bn = make_double2(b.x * i2, b.y * i2);
+		for (uint64_t m = 0; m < nm; ++m) {
+			const double2 a = to_c128(__ldg(most + m));
+			const double2 an = make_double2(a.x * i1, a.y * i1);
+			const C2 v = from_c128<C2>(cmul(an, bn));
+			__stcs(out + ((m << n2) | l), v);
+			s += sqabs(v);
+		}
+	}
+	block_sum2(dummy, s);
+	if (threadIdx.x == 0) {
+		partials[2 * blockIdx.x] = 0.0;
+		partials[2 * blockIdx.x + 1] = s;
+	}
+}
+
 /* ---- first non-zero amplitude (qops.c:57-65) ---------------------------- */
 template <typename R>
 __global__ void __launch_bounds__(256)
@@ -1869,8 +1902,24 @@ cudaError_t launch_join(int prec, const void *most, unsigned n1,
 			const Scratch &s, cudaStream_t st)
 {
 	const uint64_t size = 1ull << (n1 + n2);
-	const int blocks = grid_for(size, 256 * 4, g_num_sms * 8);
 	k_clear_flags<<<1, 1, 0, st>>>(sc_out);
+	const size_t least_bytes = (prec == DK_C128 ? 16ull : 8ull) << n2;
+	if (least_bytes > (32ull << 20) && n1 <= 10) {
+		/* least does not stay in the L2 across most amplitudes */
+		const int wb = grid_for(1ull << n2, 256 * 4, g_num_sms * 8);
+		if (prec == DK_C128)
+			k_join_wide<double><<<wb, 256, 0, st>>>((const double2 *)most, sc1,
+								(const double2 *)least, sc2, (int)n1,
+								(int)n2, (double2 *)out, s.partials);
+		else
+			k_join_wide<float><<<wb, 256, 0, st>>>((const float2 *)most, sc1,
+							       (const float2 *)least, sc2, (int)n1,
+							       (int)n2, (float2 *)out, s.partials);
+		k_finalize<<<1, 256, 0, st>>>(s.partials, wb, sc_out, sc_out, FIN_RESET, 1);
+		g_launches += 3;
+		return cudaGetLastError();
+	}
+	const int blocks = grid_for(size, 256 * 4, g_num_sms * 8);
 	if (prec == DK_C128)
 		k_join<double><<<blocks, 256, 0, st>>>((const double2 *)most, sc1,
 						      (const double2 *)least, sc2,

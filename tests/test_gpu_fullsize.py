@@ -11,7 +11,9 @@ state-vector engine, to the complex128 tolerance of the parity tests:
   register of measuring them one at a time (reference doki.c:1097-1157);
 - the reduced density matrix of qubits 0-9 is Hermitian, positive, of trace
   one, and its diagonal gives the marginals (funmatrix.c:905-1037 and
-  qops.c:72-95 evaluated on the same register).
+  qops.c:72-95 evaluated on the same register);
+- joins whose least register exceeds the L2 give the products of the inputs'
+  amplitudes and the inputs' marginals (qops.c:97-122).
 """
 from __future__ import annotations
 
@@ -132,3 +134,30 @@ def test_30q_reduced_density_properties(dk_gpu):
     a = np.arange(1024)
     for q in range(10):
         assert abs(diag[(a >> q) & 1 == 1].sum() - probs[q]) < ATOL_C128, q
+
+
+@pytest.mark.parametrize("n1,n2,prec,tol", [(3, 24, 2, ATOL_C128), (1, 29, 2, ATOL_C128),
+                                            (2, 26, 1, 1e-7)])
+def test_join_with_a_large_least_register(dk_gpu, n1, n2, prec, tol):
+    """registry_join where the least register exceeds the L2 (read once per
+    amplitude, reference qops.c:97-122): every sampled amplitude is the
+    product of the inputs' amplitudes and the result is normalised."""
+    d = dk_gpu
+    rng = W.rng_for(303 + n2)
+
+    def reg(n):
+        r = d.registry_new(n, False, prec)
+        for q in range(n):
+            r = d.registry_apply(r, d.gate_new(1, W._random_u3(rng).tolist(), False), [q],
+                                 None, None, -1, False)
+        return r
+
+    most, least = reg(n1), reg(n2)
+    j = d.registry_join(most, least, -1, False)
+    for i in _sample_indices(rng, n1 + n2, 512):
+        want = d.registry_get(most, i >> n2, False, False) * \
+            d.registry_get(least, i & ((1 << n2) - 1), False, False)
+        assert abs(d.registry_get(j, i, False, False) - want) < tol, i
+    p = d.registry_probs(j)
+    pm, pl = d.registry_probs(most), d.registry_probs(least)
+    assert np.allclose(p, list(pl) + list(pm), atol=tol * 10, rtol=0)

@@ -466,6 +466,33 @@ def test_complex64_vs_complex128_oracle(dk_gpu, orc):
     assert res_list(resa) == res_list(resb)
 
 
+@pytest.mark.parametrize("n", [8, 9, 10, 11, 13])
+def test_complex64_tile_widths_vs_complex128_oracle(dk_gpu, orc, n):
+    """complex64 sweeps on every tile width of the split-TF32 kernel (8 to 12
+    qubits) against the complex128 oracle, within the complex64 tolerance."""
+    d = dk_gpu
+    ops = random_ops(W.rng_for(90 + n), n, 120)
+    a = W.run_ops(d, d.registry_new(n, False, 1), ops)
+    b = W.run_ops(orc, orc.registry_new(n), ops)
+    va, vb = allamps(d, a), orc.registry_get_all(b)
+    assert np.max(np.abs(va - vb)) < ATOL_C64
+    fid = abs(np.vdot(vb, va)) ** 2 / (np.vdot(va, va).real * np.vdot(vb, vb).real)
+    assert fid > 1 - 1e-6
+
+
+def test_complex64_brickwork_vs_complex128_oracle(dk_gpu, orc):
+    """The benchmark's brickwork generator (chained pass pairs, conditioned
+    variants) on a complex64 register."""
+    d = dk_gpu
+    n = 14
+    c = W.scale_circuit(seed=2, n=n, depth=12, keep=6)
+    a = W.run_ops(d, d.registry_new(n, False, 1), c.ops)
+    b = W.run_ops(orc, orc.registry_new(n), c.ops)
+    va, vb = allamps(d, a), orc.registry_get_all(b)
+    assert np.max(np.abs(va - vb)) < ATOL_C64
+    assert np.allclose(d.registry_probs(a), orc.registry_probs(b), atol=ATOL_C64)
+
+
 # ------------------------------------------------------- error behaviour ----
 
 def test_device_side_errors(dk_gpu):

@@ -185,6 +185,27 @@ def finish_job(d, reg, n, keep, mask, rolls):
     return probs, res, mat
 
 
+def tensor_roofline(entry_amps, sweep_s, c64, clk, steps):
+    """Tensor-pipe work of the timed sweeps.  One matrix entry applied to one
+    amplitude is 24 FP64 MMA FMA (complex128: three real m8n8k4 products of
+    two k-steps per 64 amplitudes) or 96 TF32 MMA FMA (complex64: six m16n8k8
+    MMAs per 64 amplitudes).  The FP64 peak is the MMA op rate ncu reports
+    (sm__ops_path_tensor_src_fp64: 128 per SM per cycle) x SMs x the median SM
+    clock of the run; no TF32 figure is measured, so complex64 has none."""
+    import torch
+    fma = entry_amps * (96 if c64 else 24)
+    achieved = 2.0 * fma / max(sweep_s, 1e-12) / 1e12
+    out = {"pipe": "tf32 mma.sync m16n8k8" if c64 else "fp64 mma.sync m8n8k4",
+           "achieved": achieved, "unit": "TFLOP/s", "flops_per_step": 2.0 * fma / steps}
+    if not c64:
+        mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        peak = 128.0 * sms * mhz * 1e6 / 1e12
+        out.update({"peak": peak, "frac": achieved / peak,
+                    "peak_kind": f"ncu FP64 MMA op rate 128/SM/cycle x {sms} SMs x {mhz:g} MHz"})
+    return out
+
+
 def engine_arm(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -295,6 +316,9 @@ def engine_arm(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": (io1["h2d_bytes"] - io0["h2d_bytes"]) // args.steps,
                 "d2h_bytes_per_step": (io1["d2h_bytes"] - io0["d2h_bytes"]) // args.steps},
+        "tensor_roofline": tensor_roofline(st1["mma_entry_amplitudes"] -
+                                           st0["mma_entry_amplitudes"],
+                                           sweep_ms / 1e3, c64, clk, args.steps),
         "gpu_launches": st1["kernel_launches"] - st0["kernel_launches"],
         "clocks": clk,
         "fusion": not args.no_fusion,

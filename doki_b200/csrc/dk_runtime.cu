@@ -55,6 +55,8 @@ struct Ctx {
 	int tensor = 0; /* tensor-core sweeps: 0 planner default (on), < 0 off */
 	int low_bits = -1; /* qubits always in a sweep's tile: < 0 planner default */
 	std::atomic<unsigned long long> sweeps{ 0 }, gates{ 0 }, h2d{ 0 }, d2h{ 0 };
+	/* tensor sweeps: sum of matrix entries x register amplitudes */
+	std::atomic<unsigned long long> mma_entry_amps{ 0 };
 	char err[256] = { 0 };
 };
 
@@ -336,6 +338,15 @@ int flush(dk_state *s)
 			e = dk::launch_sweep(prec, cur, dst->d, dblob + stp.prog_off, hp,
 					     cur_sc, dst->sc, CUR.scratch, g.num_sms, CUR.st);
 			g.sweeps++;
+			if (hp->mode == DK_SWEEP_TENSOR) {
+				const dk_pass_desc *pd = (const dk_pass_desc *)(plan.blob +
+										 stp.prog_off +
+										 hp->pass_off);
+				unsigned long long entries = 0;
+				for (int p = 0; p < hp->npass; ++p)
+					entries += (unsigned long long)(pd[p].g1 - pd[p].g0);
+				g.mma_entry_amps += entries << n;
+			}
 			g.gates += (unsigned long long)stp.ngates;
 		} else {
 			const dk_flat_op &op = ops[stp.op_index];
@@ -1356,6 +1367,13 @@ int dk_get_stats(uint64_t *kernel_launches, uint64_t *sweeps, uint64_t *gates_ap
 		*sweeps = g.sweeps;
 	if (gates_applied)
 		*gates_applied = g.gates;
+	return DK_OK;
+}
+
+int dk_get_mma_stats(uint64_t *entry_amplitudes)
+{
+	if (entry_amplitudes)
+		*entry_amplitudes = g.mma_entry_amps;
 	return DK_OK;
 }
 

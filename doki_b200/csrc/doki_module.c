@@ -1276,13 +1276,15 @@ static PyObject *doki_engine_set_fusion(PyObject *self, PyObject *args)
 
 static PyObject *doki_engine_stats(PyObject *self, PyObject *args)
 {
-	uint64_t l = 0, s = 0, g = 0, hi = 0, ho = 0;
+	uint64_t l = 0, s = 0, g = 0, hi = 0, ho = 0, me = 0;
 	dk_get_stats(&l, &s, &g);
 	dk_get_io_stats(&hi, &ho);
-	return Py_BuildValue("{s:K,s:K,s:K,s:K,s:K}", "kernel_launches",
+	dk_get_mma_stats(&me);
+	return Py_BuildValue("{s:K,s:K,s:K,s:K,s:K,s:K}", "kernel_launches",
 			     (unsigned long long)l, "sweeps", (unsigned long long)s, "gates",
 			     (unsigned long long)g, "h2d_bytes", (unsigned long long)hi,
-			     "d2h_bytes", (unsigned long long)ho);
+			     "d2h_bytes", (unsigned long long)ho, "mma_entry_amplitudes",
+			     (unsigned long long)me);
 }
 
 static PyObject *doki_registry_compare(PyObject *self, PyObject *args)

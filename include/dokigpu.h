@@ -155,6 +155,12 @@ int dk_set_fusion(int enable);
  * sweeps executed and gates applied by them.  Any pointer may be NULL. */
 int dk_get_stats(uint64_t *kernel_launches, uint64_t *sweeps,
 		 uint64_t *gates_applied);
+/* Tensor-core sweep work since dk_init: the sum over launched tensor sweeps
+ * of (8x8 matrix entries in the sweep) x (amplitudes of the register).  One
+ * entry-amplitude is 24 FMA on FP64 MMAs (complex128, Gauss form: 3 real
+ * products of 2 m8n8k4 k-steps per 64 amplitudes) or 96 TF32 MMA FMA
+ * (complex64: 6 m16n8k8 MMAs per 64 amplitudes). */
+int dk_get_mma_stats(uint64_t *entry_amplitudes);
 /* Bytes copied host->device and device->host by this library since dk_init. */
 int dk_get_io_stats(uint64_t *h2d_bytes, uint64_t *d2h_bytes);
 /* Execute the gates queued on `s` now (normally deferred to the next read). */

@@ -520,3 +520,16 @@ def test_device_side_errors(dk_gpu):
     assert msgs["roll"] == msgs["short"] == "roll not in interval [0, 1)!"
     r0, res = d.registry_measure(r, 0, [], 1, False)
     assert res == [None, None, None] and r0 is not None
+
+
+def test_tensor_work_counter(dk_gpu):
+    """engine_stats()["mma_entry_amplitudes"] grows by (matrix entries) x
+    (register amplitudes) for each tensor sweep, so it is a multiple of 2^n."""
+    d = dk_gpu
+    n = 14
+    before = d.engine_stats()["mma_entry_amplitudes"]
+    c = W.scale_circuit(seed=2, n=n, depth=6, keep=6)
+    r = W.run_ops(d, d.registry_new(n, False), c.ops)
+    d.registry_flush(r)
+    grown = d.engine_stats()["mma_entry_amplitudes"] - before
+    assert grown > 0 and grown % (1 << n) == 0

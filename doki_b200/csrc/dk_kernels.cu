@@ -1026,6 +1026,62 @@ __global__ void __launch_bounds__(256)
 	}
 }
 
+/* Joint distribution of k <= 4 measured qubits in one contiguous pass over
+ * the register (coalesced like k_marginals): thread t adds |amp_i|^2 to its
+ * own shared-memory column hist[bin(i)][t], no atomics, and the columns of
+ * each bin are added in a fixed order.  Writes partials[bin * gridDim.x +
+ * block] as k_joint does, for k_joint_finalize.  k_joint instead gives each
+ * bin its own blocks, which gather the bin's amplitudes; with a low measured
+ * qubit those gathers use part of every 32-byte sector and every bin re-reads
+ * the same sectors. */
+constexpr int kJointSmallBins = 16;
+constexpr uint64_t kJointSeg = 4096; /* amplitudes per block step, 16 per thread */
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_joint_small(const typename CT<R>::T *__restrict__ in, uint64_t size, uint32_t qpack,
+		      int k, double *partials)
+{
+	__shared__ double hist[kJointSmallBins][256];
+	const uint32_t t = threadIdx.x;
+	const int nb = 1 << k;
+	for (int b = 0; b < nb; ++b)
+		hist[b][t] = 0.0; /* each thread only ever touches its own column */
+	int qs[4];
+#pragma unroll
+	for (int j = 0; j < 4; ++j)
+		qs[j] = (int)((qpack >> (8 * j)) & 0xffu);
+	for (uint64_t base = (uint64_t)blockIdx.x * kJointSeg; base < size;
+	     base += (uint64_t)gridDim.x * kJointSeg) {
+		double p[16];
+#pragma unroll
+		for (int u = 0; u < 16; ++u)
+			p[u] = sqabs(__ldcs(in + base + t + 256u * u));
+#pragma unroll
+		for (int u = 0; u < 16; ++u) {
+			const uint64_t i = base + t + 256u * u;
+			uint32_t b = 0;
+#pragma unroll
+			for (int j = 0; j < 4; ++j)
+				if (j < k)
+					b |= (uint32_t)((i >> qs[j]) & 1u) << j;
+			hist[b][t] += p[u];
+		}
+	}
+	__syncthreads();
+	const uint32_t w = t >> 5, l = t & 31u;
+	for (int b = (int)w; b < nb; b += (int)(blockDim.x >> 5)) {
+		double v = 0.0;
+		for (uint32_t c = l; c < 256u; c += 32u)
+			v += hist[b][c];
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1)
+			v += __shfl_xor_sync(0xffffffffu, v, o);
+		if (l == 0)
+			partials[(uint64_t)b * gridDim.x + blockIdx.x] = v;
+	}
+}
+
 /* joint[bin] = sum of its chunks, in order */
 __global__ void __launch_bounds__(256)
 	k_joint_finalize(const double *partials, uint64_t nchunk, double *joint)
@@ -1871,15 +1927,35 @@ cudaError_t launch_measure_joint(int prec, const void *in, void *out, unsigned n
 	double *part = s.partials;
 	double *joint = s.partials + kJointPartials;
 	uint64_t *vbits = reinterpret_cast<uint64_t *>(s.u64 + 1);
-	uint64_t gx = nchunk < (uint64_t)g_num_sms * 8 ? nchunk : (uint64_t)g_num_sms * 8;
-	dim3 grid((unsigned)gx, (unsigned)nbins);
-	if (prec == DK_C128)
-		k_joint<double><<<grid, 256, 0, st>>>((const double2 *)in, runs, mask, per_bin,
-						      chunk, nchunk, part);
-	else
-		k_joint<float><<<grid, 256, 0, st>>>((const float2 *)in, runs, mask, per_bin, chunk,
-						     nchunk, part);
-	k_joint_finalize<<<(unsigned)nbins, 256, 0, st>>>(part, nchunk, joint);
+	if (k <= 4 && n >= 12) {
+		/* one contiguous pass, 2048 blocks at most */
+		uint32_t qpack = 0;
+		int j = 0;
+		for (unsigned q = 0; q < n; ++q)
+			if ((mask >> q) & 1u)
+				qpack |= q << (8 * j++);
+		const uint64_t size = 1ull << n;
+		uint64_t nb = size / kJointSeg;
+		if (nb > 2048)
+			nb = 2048;
+		if (prec == DK_C128)
+			k_joint_small<double><<<(unsigned)nb, 256, 0, st>>>((const double2 *)in, size,
+									    qpack, k, part);
+		else
+			k_joint_small<float><<<(unsigned)nb, 256, 0, st>>>((const float2 *)in, size,
+									   qpack, k, part);
+		k_joint_finalize<<<(unsigned)nbins, 256, 0, st>>>(part, nb, joint);
+	} else {
+		uint64_t gx = nchunk < (uint64_t)g_num_sms * 8 ? nchunk : (uint64_t)g_num_sms * 8;
+		dim3 grid((unsigned)gx, (unsigned)nbins);
+		if (prec == DK_C128)
+			k_joint<double><<<grid, 256, 0, st>>>((const double2 *)in, runs, mask,
+							      per_bin, chunk, nchunk, part);
+		else
+			k_joint<float><<<grid, 256, 0, st>>>((const float2 *)in, runs, mask,
+							     per_bin, chunk, nchunk, part);
+		k_joint_finalize<<<(unsigned)nbins, 256, 0, st>>>(part, nchunk, joint);
+	}
 	k_decide_joint<<<1, 32, 0, st>>>(joint, k, rolls_dev, flags_dev, vbits, mask, sc_in, sc_out);
 	g_launches += 3;
 	if (out != nullptr) {

@@ -276,7 +276,9 @@ def test_measure_joint_vs_oracle(dk_gpu, orc, n, prec):
     b = W.run_ops(orc, orc.registry_new(n), ops)
     masks = [1, 1 << (n - 1), 0b1011, (1 << (n - 1)) | 1 | (1 << (n // 2)),
              sum(1 << int(q) for q in rng.choice(n, size=min(12, n), replace=False)),
-             sum(1 << int(q) for q in rng.choice(n, size=5, replace=False))]
+             sum(1 << int(q) for q in rng.choice(n, size=5, replace=False)),
+             sum(1 << int(q) for q in rng.choice(n, size=6, replace=False)),
+             0b1111111]
     for mask in masks:
         for _ in range(3):
             rolls = rng.random(bin(mask).count("1")).tolist()

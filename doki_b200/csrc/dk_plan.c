@@ -402,18 +402,46 @@ static void chain_pair(dk_pass_desc *pa, dk_pass_desc *pb, uint32_t PA, uint32_t
  * lane bits.  A warp then touches the same tile slots in every pass of the
  * phase, so consecutive passes only need a warp barrier.  `need[i]` are the
  * target bits of pass i; they are filled up to DK_PASS_BITS from the phase's
- * union first (keeping it small), W is picked from the rest. */
+ * union first (keeping it small), W is picked from the rest.
+ *
+ * Tensor sweeps: two neighbouring single-entry passes whose target bits are
+ * disjoint chain in registers when their filled bit sets are disjoint too.
+ * Such pairs are marked first (greedily from the front, which gives the most
+ * pairs on a path) and filled from disjoint bits; the phase's union grows to
+ * 2 * DK_PASS_BITS bits when it holds fewer, which still leaves the wbits
+ * warp bits and the 2 lane bits a chained pair maps besides its 6 pass bits
+ * (m - wbits = DK_PASS_BITS + 5). */
 static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, int wbits,
 			int res, int tensor, const phase_ctx *cx,
 			uint8_t (*pbits)[DK_PASS_BITS])
 {
 	uint32_t F = 0, pmask[64];
+	uint8_t pair[64] = { 0 }; /* pass i chains with pass i + 1 */
 	for (int i = 0; i < cnt; i++)
 		F |= need[i];
 	for (int bit = m - 1; popc(F) < DK_PASS_BITS && bit >= 0; bit--)
 		F |= 1u << bit;
+	if (tensor && cx && wbits >= 0 && m - wbits >= 2 * DK_PASS_BITS) {
+		for (int i = 0; i + 1 < cnt; i++) {
+			if ((need[i] & need[i + 1]) || !single_entry(cx, &pd[i], need[i]) ||
+			    !single_entry(cx, &pd[i + 1], need[i + 1]))
+				continue;
+			for (int bit = m - 1; popc(F) < 2 * DK_PASS_BITS && bit >= 0; bit--)
+				F |= 1u << bit;
+			pair[i] = 1;
+			i++;
+		}
+	}
 	for (int i = 0; i < cnt; i++) {
 		uint32_t P = need[i];
+		if (pair[i] || (i > 0 && pair[i - 1])) {
+			/* a chained pair: fillers avoid both passes' bits */
+			const int j = pair[i] ? i + 1 : i - 1;
+			const uint32_t avoid = need[j] | (pair[i] ? 0u : pmask[j]);
+			for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
+				if ((F & (1u << bit)) && !(avoid & (1u << bit)))
+					P |= 1u << bit;
+		}
 		for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
 			if (F & (1u << bit))
 				P |= 1u << bit;
@@ -451,8 +479,10 @@ static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, 
 	}
 	if (tensor) {
 		for (int i = 0; i < cnt; i++) {
-			/* a pair of single-entry passes on disjoint bits chains */
+			/* a pair of single-entry passes on disjoint bits chains
+			 * (never one that would split a pair marked above) */
 			if (cx && wbits >= 0 && i + 1 < cnt && !(pmask[i] & pmask[i + 1]) &&
+			    (pair[i] || !pair[i + 1]) &&
 			    single_entry(cx, &pd[i], pmask[i]) &&
 			    single_entry(cx, &pd[i + 1], pmask[i + 1])) {
 				chain_pair(&pd[i], &pd[i + 1], pmask[i], pmask[i + 1], W, m, res,

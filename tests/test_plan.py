@@ -462,3 +462,43 @@ def test_chained_pairs_keep_the_mma_layout(lib, prec, n):
             assert tb[:3] == pass_bits(p)
             assert ta[3:] == tb[3:]
     assert chained > 0 and chained * 2 <= total
+
+
+def test_disjoint_neighbour_passes_chain(lib, orc):
+    """Two neighbouring single-entry passes whose target bits are disjoint
+    chain even when the phase's bits would otherwise fill the second pass with
+    a bit of the first: U3 on qubits 4-6 form one pass and U3 on 7-8 the next;
+    filling the second from the phase's five bits alone would take bit 6, so
+    the planner widens the phase to six bits and fills it with another."""
+    n = 12
+    rng = W.rng_for(4242)
+    ops = [W.Op(W.u3(*rng.uniform(0, 2 * np.pi, 3)), [q]) for q in (4, 5, 6, 7, 8)]
+    steps, blob = build_plan(lib, ops, n)
+    assert len(steps) == 1 and steps[0][0] == 1
+    h = np.frombuffer(blob, HDR, 1, steps[0][1])[0]
+    passes = np.frombuffer(blob, PASS, int(h["npass"]), steps[0][1] + int(h["pass_off"]))
+    assert len(passes) == 2
+    assert int(passes[0]["flags"]) & 4
+    assert {4, 5, 6} == set(pass_bits(passes[0]))
+    assert {7, 8} <= set(pass_bits(passes[1]))
+    assert not set(pass_bits(passes[0])) & set(pass_bits(passes[1]))
+    psi0 = np.zeros(1 << n, dtype=np.complex128)
+    psi0[0] = 1
+    got, _ = run_plan(lib, ops, n, psi0)
+    want = oracle_run(orc, ops, n)
+    assert np.allclose(got, want, atol=1e-12)
+
+
+def test_scale_circuit_chains_most_passes(lib):
+    """On the 30-qubit depth-40 workload more than half of the tensor passes
+    run as chained pairs (the remaining ones hold several entries, overlap
+    their neighbour, or are the odd pass of a sweep)."""
+    c = W.scale_circuit(seed=2, n=30, depth=40)
+    steps, blob = build_plan(lib, c.ops, 30)
+    chained = total = 0
+    for kind, off, _ in steps:
+        h = np.frombuffer(blob, HDR, 1, off)[0]
+        passes = np.frombuffer(blob, PASS, int(h["npass"]), off + int(h["pass_off"]))
+        total += len(passes)
+        chained += 2 * sum(1 for p in passes if int(p["flags"]) & 4)
+    assert chained > total // 2, (chained, total)

@@ -38,7 +38,13 @@ void dk_plan_default_limits(int prec, unsigned n, dk_plan_limits *lim)
 	if ((int)n < m)
 		m = (int)n;
 	lim->tile_bits = m;
-	lim->low_bits = m < 4 ? m : 4;
+	/* pinned low qubits: tensor sweeps pin 2 (contiguous runs of 64 bytes
+	 * for complex128, 32 for complex64): the freer tile choice gives fewer
+	 * sweeps (30 qubits, depth 40: 65 against 83), which outweighs the
+	 * slower streaming of shorter runs at both precisions.  Scalar sweeps
+	 * pin 4. */
+	const int low = lim->tensor >= 0 ? 2 : 4;
+	lim->low_bits = m < low ? m : low;
 	lim->max_gates = 512;
 	lim->max_passes = 512;
 	lim->max_mat = 4096; /* complex entries: <= 64 KiB of a sweep's shared memory */

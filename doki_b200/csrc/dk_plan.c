@@ -814,12 +814,35 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	 * lanes).  Narrower tiles fill each pass with the highest free bits. */
 	const int wbits = m - DK_PASS_BITS - 5;
 	const phase_ctx cx = { ops, order, loc_of, n };
+	/* tensor sweeps: neighbouring passes that can chain (disjoint target
+	 * bits, one entry each), marked greedily from the front as build_phase
+	 * does; a phase is cut before such a pair rather than between its two
+	 * passes, trading a block barrier for a chained pair */
+	uint8_t *pairs = (uint8_t *)calloc((size_t)(npass ? npass : 1), 1);
+	if (!pairs) {
+		free(rem);
+		free(defer);
+		free(order);
+		free(passes);
+		free(pbits);
+		free(need);
+		return -1;
+	}
+	if (fold->tensor && wbits >= 0 && m - wbits >= 2 * DK_PASS_BITS)
+		for (int i = 0; i + 1 < npass; i++)
+			if (!(need[i] & need[i + 1]) && single_entry(&cx, &passes[i], need[i]) &&
+			    single_entry(&cx, &passes[i + 1], need[i + 1])) {
+				pairs[i] = 1;
+				i++;
+			}
 	for (int p0 = 0; p0 < npass;) {
 		int p1 = p0 + 1;
 		if (wbits >= 0) {
 			uint32_t U = need[p0];
 			while (p1 < npass && p1 - p0 < 64 && popc(U | need[p1]) <= m - wbits)
 				U |= need[p1++];
+			if (p1 < npass && p1 - 1 > p0 && pairs[p1 - 1])
+				p1--;
 			build_phase(&passes[p0], &need[p0], p1 - p0, m, wbits, res, fold->tensor,
 				    fold->tensor ? &cx : NULL, &pbits[p0]);
 		} else {
@@ -834,6 +857,7 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 		}
 		p0 = p1;
 	}
+	free(pairs);
 
 	/* Gate-list entries.  Scalar sweeps: a run of consecutive gates of a
 	 * pass that act only on the pass's bits (targets and controls) and on

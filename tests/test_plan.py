@@ -502,3 +502,30 @@ def test_scale_circuit_chains_most_passes(lib):
         total += len(passes)
         chained += 2 * sum(1 for p in passes if int(p["flags"]) & 4)
     assert chained > total // 2, (chained, total)
+
+
+def test_phases_keep_chainable_pairs_together(lib, orc):
+    """A warp phase grows while its passes fit in m - wbits tile bits; when
+    that would end it between two passes that can chain, the planner ends it
+    one pass earlier (one more block barrier, one more chained pair).  On this
+    12-qubit sweep of CZ and U3 gates both pass pairs chain."""
+    n = 12
+    rng = W.rng_for(31)
+
+    def u3():
+        return W.u3(*rng.uniform(0, 2 * np.pi, 3))
+
+    ops = [W.Op(W.Z.copy(), [0], {5}), W.Op(W.Z.copy(), [2], {3}), W.Op(W.Z.copy(), [3], {4}),
+           W.Op(u3(), [9]), W.Op(W.Z.copy(), [1], {3}), W.Op(u3(), [6]),
+           W.Op(W.Z.copy(), [0], {2}), W.Op(u3(), [3]), W.Op(u3(), [6]), W.Op(u3(), [9]),
+           W.Op(u3(), [11])]
+    steps, blob = build_plan(lib, ops, n)
+    assert len(steps) == 1 and steps[0][0] == 1
+    h = np.frombuffer(blob, HDR, 1, steps[0][1])[0]
+    passes = np.frombuffer(blob, PASS, int(h["npass"]), steps[0][1] + int(h["pass_off"]))
+    assert sum(2 for p in passes if int(p["flags"]) & 4) == 4
+    psi0 = W.rng_for(5).normal(size=1 << n) + 1j * W.rng_for(6).normal(size=1 << n)
+    got, _ = run_plan(lib, ops, n, psi0)
+    reg = orc.registry_new_data(n, psi0)
+    want = orc.registry_get_all(W.run_ops(orc, reg, ops))
+    assert np.allclose(got / np.linalg.norm(got), want, atol=1e-12)

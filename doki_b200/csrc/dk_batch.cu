@@ -309,6 +309,7 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 		   const uint64_t *op_anticontrols, const uint64_t *op_matrix,
 		   const double *matrices, int tile_bits, dk_batch **out)
 {
+	DK_TRACE();
 	if (!out || (precision != DK_C64 && precision != DK_C128) || !num_qubits ||
 	    !keep_qubits || !op_start || (num_circuits == 0))
 		return DK_ERR_ARG;
@@ -530,6 +531,7 @@ static cudaError_t batch_enqueue(dk_batch *b, int keep_states)
 
 int dk_batch_run(dk_batch *b, int keep_states)
 {
+	DK_TRACE();
 	if (!b)
 		return DK_ERR_ARG;
 	keep_states = keep_states ? 1 : 0;
@@ -574,6 +576,7 @@ int dk_batch_run(dk_batch *b, int keep_states)
 
 int dk_batch_sync(dk_batch *b)
 {
+	DK_TRACE();
 	if (!b)
 		return DK_ERR_ARG;
 	cudaError_t e = cudaStreamSynchronize(b->st);
@@ -584,6 +587,7 @@ void *dk_batch_stream(dk_batch *b) { return b ? (void *)b->st : nullptr; }
 
 int dk_batch_rho(dk_batch *b, unsigned circuit, double *out)
 {
+	DK_TRACE();
 	if (!b || !out || circuit >= b->ncirc)
 		return DK_ERR_ARG;
 	const size_t cnt = 1ull << (2 * b->keep[circuit]);
@@ -596,6 +600,7 @@ int dk_batch_rho(dk_batch *b, unsigned circuit, double *out)
 
 int dk_batch_rho_all(dk_batch *b, double *out, uint64_t *offsets)
 {
+	DK_TRACE();
 	if (!b || !out)
 		return DK_ERR_ARG;
 	cudaError_t e = cudaMemcpyAsync(out, b->drho, 16 * b->rho_elems, cudaMemcpyDeviceToHost,
@@ -612,6 +617,7 @@ uint64_t dk_batch_rho_elems(const dk_batch *b) { return b ? b->rho_elems : 0; }
 
 int dk_batch_state(dk_batch *b, unsigned circuit, double *out)
 {
+	DK_TRACE();
 	if (!b || !out || circuit >= b->ncirc)
 		return DK_ERR_ARG;
 	const size_t cnt = 1ull << b->n[circuit];

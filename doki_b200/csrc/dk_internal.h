@@ -232,6 +232,20 @@ int dk_gate_classify(const struct dk_gate *g);
 
 #ifdef __cplusplus
 }
+
+#include <nvtx3/nvToolsExt.h>
+
+/* An NVTX range over one C-ABI call, named after the function, so that a
+ * profiler timeline (ncu --nvtx, Nsight Systems) shows which call launched
+ * which kernels.  NVTX is header-only: with no tool attached a push or pop
+ * is a check of one function pointer. */
+struct dk_nvtx_scope {
+	explicit dk_nvtx_scope(const char *name) { nvtxRangePushA(name); }
+	~dk_nvtx_scope() { nvtxRangePop(); }
+	dk_nvtx_scope(const dk_nvtx_scope &) = delete;
+	dk_nvtx_scope &operator=(const dk_nvtx_scope &) = delete;
+};
+#define DK_TRACE() dk_nvtx_scope dk_nvtx_scope_(__func__)
 #endif
 
 #endif /* DK_INTERNAL_H_ */

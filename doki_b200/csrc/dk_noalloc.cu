@@ -39,6 +39,7 @@ double *g_noalloc_addr[kMaxDevices] = { nullptr };
 extern "C" int dk_marginals_noalloc(const void *amps, unsigned num_qubits, int precision,
 				    double *out, void *stream)
 {
+	DK_TRACE();
 	if (!amps || !out || (precision != DK_C64 && precision != DK_C128) || num_qubits == 0)
 		return DK_ERR_ARG;
 	if (num_qubits > DK_NOALLOC_MAX_QUBITS)

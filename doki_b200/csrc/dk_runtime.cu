@@ -251,6 +251,7 @@ int flush(dk_state *s)
 {
 	if (!s->pending)
 		return DK_OK;
+	DK_TRACE();
 	const unsigned n = s->n;
 	const int prec = s->prec;
 	const uint32_t cnt = s->pending->depth;
@@ -491,6 +492,7 @@ const char *dk_last_cuda_error(void) { return g.err; }
 
 int dk_init(int device)
 {
+	DK_TRACE();
 	std::lock_guard<std::mutex> lk(g.init_mu);
 	if (g.inited.load())
 		return DK_OK;
@@ -616,6 +618,7 @@ void dk_gate_free(dk_gate *gate)
 
 int dk_state_new(unsigned num_qubits, int precision, dk_state **out)
 {
+	DK_TRACE();
 	if (ensure_init() != DK_OK)
 		return ensure_init();
 	SlotLock lk(t_slot);
@@ -649,6 +652,7 @@ int dk_state_new(unsigned num_qubits, int precision, dk_state **out)
 int dk_state_from_host(unsigned num_qubits, int precision, const double *values,
 		       dk_state **out)
 {
+	DK_TRACE();
 	if (ensure_init() != DK_OK)
 		return ensure_init();
 	SlotLock lk(t_slot);
@@ -697,6 +701,7 @@ int dk_state_from_host(unsigned num_qubits, int precision, const double *values,
 
 int dk_state_clone(dk_state *src, dk_state **out)
 {
+	DK_TRACE();
 	SlotLock lk(src ? src->slot : t_slot);
 	int rc = check_live(src);
 	if (rc)
@@ -759,6 +764,7 @@ int dk_apply_gate(dk_state *in, const dk_gate *gate, const unsigned *targets,
 		  unsigned num_controls, const unsigned *anticontrols,
 		  unsigned num_anticontrols, dk_state **out)
 {
+	DK_TRACE();
 	SlotLock lk(in ? in->slot : t_slot);
 	int rc = check_live(in);
 	if (rc)
@@ -816,6 +822,7 @@ int dk_apply_gate(dk_state *in, const dk_gate *gate, const unsigned *targets,
 
 int dk_get_amplitude(dk_state *s, uint64_t id, double *re, double *im)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
@@ -852,6 +859,7 @@ int dk_get_amplitude(dk_state *s, uint64_t id, double *re, double *im)
 
 int dk_get_amplitudes(dk_state *s, uint64_t first, uint64_t count, double *out)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
@@ -885,6 +893,7 @@ int dk_get_amplitudes(dk_state *s, uint64_t first, uint64_t count, double *out)
 
 int dk_global_phase(dk_state *s, double *phase)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
@@ -928,6 +937,7 @@ int dk_global_phase(dk_state *s, double *phase)
 
 int dk_marginals(dk_state *s, double *p)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
@@ -960,6 +970,7 @@ int dk_marginals(dk_state *s, double *p)
 
 int dk_probability(dk_state *s, unsigned target, double *p)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = check_live(s);
 	if (rc)
@@ -977,6 +988,7 @@ int dk_probability(dk_state *s, unsigned target, double *p)
 int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 		    unsigned num_rolls, int8_t *results, dk_state **out)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
@@ -1159,6 +1171,7 @@ int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 int dk_measure(dk_state *s, unsigned target, double roll, int *result,
 	       dk_state **out)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = check_live(s);
 	if (rc)
@@ -1175,6 +1188,7 @@ int dk_measure(dk_state *s, unsigned target, double roll, int *result,
 
 int dk_join(dk_state *most, dk_state *least, dk_state **out)
 {
+	DK_TRACE();
 	if (!most || !least)
 		return DK_ERR_ARG;
 	int rc;
@@ -1229,6 +1243,7 @@ int dk_join(dk_state *most, dk_state *least, dk_state **out)
 
 int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
@@ -1302,6 +1317,7 @@ int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)
 int dk_reduced_density_elem(dk_state *s, uint64_t keep_mask, uint64_t i,
 			    uint64_t j, double *re, double *im)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = prepare_read(s);
 	if (rc)
@@ -1323,6 +1339,7 @@ int dk_reduced_density_elem(dk_state *s, uint64_t keep_mask, uint64_t i,
 
 int dk_compare_states(dk_state *x, dk_state *y, double *fidelity, double *max_amp_err)
 {
+	DK_TRACE();
 	if (!x || !y || x->n != y->n)
 		return DK_ERR_ARG;
 	if (x->slot != y->slot) {
@@ -1389,6 +1406,7 @@ int dk_get_io_stats(uint64_t *h2d_bytes, uint64_t *d2h_bytes)
 
 int dk_state_flush(dk_state *s)
 {
+	DK_TRACE();
 	SlotLock lk(s ? s->slot : t_slot);
 	int rc = check_live(s);
 	if (rc)
@@ -1411,6 +1429,7 @@ void *dk_stream(void)
 
 int dk_sync(void)
 {
+	DK_TRACE();
 	if (!g.inited.load())
 		return DK_OK;
 	const int ns = g.nslots.load();

@@ -30,6 +30,10 @@ C_SOURCES = ["dk_plan.c"]
 HEADERS = ["dk_internal.h", "dk_kernels.h", "dk_device.cuh"]
 
 LIB = os.path.join(HERE, "libdokigpu.so")
+# Debug build: the kernels check every index they compute
+# (-DDK_DEBUG_CHECKS) and export dk_debug_checks; only dk_kernels.cu differs.
+LIB_DBG = os.path.join(HERE, "libdokigpu_dbg.so")
+DBG_SOURCE = "dk_kernels.cu"
 EXT = os.path.join(HERE, "doki" + sysconfig.get_config_var("EXT_SUFFIX"))
 
 
@@ -68,6 +72,14 @@ def build(force: bool = False, verbose: bool = False) -> None:
         [os.path.join(INC, "dokigpu.h")]
     objs = []
     nvcc = _nvcc()
+    dsrc = os.path.join(CSRC, DBG_SOURCE)
+    dobj = os.path.join(OBJ, DBG_SOURCE + ".dbg.o")
+    dproc = None
+    if force or _stale(dobj, [dsrc] + hdrs):
+        # compiled beside the release objects, in parallel with them
+        dproc = subprocess.Popen([nvcc, *ARCH, *NVCC_FLAGS, "-DDK_DEBUG_CHECKS", "-c", dsrc,
+                                  "-o", dobj], stdout=subprocess.PIPE,
+                                 stderr=subprocess.PIPE, text=True)
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src + ".o")
@@ -89,6 +101,15 @@ def build(force: bool = False, verbose: bool = False) -> None:
     if force or _stale(LIB, objs):
         _run([nvcc, *ARCH, "-shared", "-o", LIB, *objs,
               "-Xlinker", "-rpath=/usr/local/cuda/lib64"])
+    if dproc is not None:
+        out, err = dproc.communicate()
+        if dproc.returncode != 0:
+            sys.stderr.write(out + err)
+            raise RuntimeError(f"build step failed: debug {DBG_SOURCE} ({dproc.returncode})")
+    dobjs = [dobj if o.endswith(DBG_SOURCE + ".o") else o for o in objs]
+    if force or _stale(LIB_DBG, dobjs):
+        _run([nvcc, *ARCH, "-shared", "-o", LIB_DBG, *dobjs,
+              "-Xlinker", "-rpath=/usr/local/cuda/lib64", "-Xlinker", "-Bsymbolic"])
     msrc = os.path.join(CSRC, "doki_module.c")
     if force or _stale(EXT, [msrc, LIB, os.path.join(INC, "dokigpu.h")]):
         pyinc = sysconfig.get_paths()["include"]

@@ -230,6 +230,11 @@ int dk_plan_build(const dk_flat_op *ops, int nops, unsigned n, int prec,
 void dk_plan_free(dk_plan *plan);
 int dk_gate_classify(const struct dk_gate *g);
 
+/* Debug builds only (libdokigpu_dbg.so, -DDK_DEBUG_CHECKS): the first failed
+ * kernel index check since the last reset, 0 if none (site in bits 56-63,
+ * index in bits 0-55). */
+int dk_debug_checks(uint64_t *first_failure, int reset);
+
 #ifdef __cplusplus
 }
 

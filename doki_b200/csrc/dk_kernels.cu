@@ -19,6 +19,36 @@
 namespace dk {
 namespace {
 
+/* Debug builds (-DDK_DEBUG_CHECKS, libdokigpu_dbg.so): the table-driven
+ * kernels check every global and shared-memory index they compute.  A failed
+ * check records its site (bits 56-63) and index (bits 0-55) in g_dk_check --
+ * the first failure wins -- and the access is skipped; nothing traps, so the
+ * context stays usable and dk_debug_checks() reads the record.  Release
+ * builds compile the checks away. */
+#ifdef DK_DEBUG_CHECKS
+__device__ unsigned long long g_dk_check;
+__device__ __forceinline__ bool dk_in_bounds(uint64_t i, uint64_t lim, unsigned site)
+{
+	if (i < lim)
+		return true;
+	atomicCAS(&g_dk_check, 0ull,
+		  ((unsigned long long)site << 56) | (i & ((1ull << 56) - 1ull)));
+	return false;
+}
+#define DK_IN_BOUNDS(i, lim, site) dk_in_bounds((uint64_t)(i), (uint64_t)(lim), (site))
+#else
+#define DK_IN_BOUNDS(i, lim, site) true
+#endif
+enum {
+	CHK_LOAD_SMEM = 1, /* tile slot of a global -> shared copy */
+	CHK_LOAD_GLOBAL = 2, /* amplitude index read from the register */
+	CHK_GATHER = 3, /* tile slot read by a pass */
+	CHK_SCATTER = 4, /* tile slot written by a pass */
+	CHK_READOUT = 5, /* tile slot read for the write-back */
+	CHK_STORE = 6, /* amplitude index written to the register */
+	CHK_COLLAPSE = 7 /* amplitude index read by a collapse */
+};
+
 /* ---- fused sweep ------------------------------------------------------- */
 
 
@@ -128,15 +158,21 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 		}
 		return ntiles;
 	};
+	[[maybe_unused]] const uint64_t nglob = 1ull << h->n;
 	auto prefetch = [&](uint64_t base, C2 *buf) {
 		const uint64_t bo = base | off_t;
 #pragma unroll
 		for (int r = 0; r < NA; ++r) {
-			C2 *dst = buf + (stid ^ sro[r]);
+			const uint32_t so = stid ^ sro[r];
+			const uint64_t gi = bo | soff[r];
+			if (!DK_IN_BOUNDS(so, tn_amp, CHK_LOAD_SMEM) ||
+			    !DK_IN_BOUNDS(gi, nglob, CHK_LOAD_GLOBAL))
+				continue;
+			C2 *dst = buf + so;
 			if (sizeof(C2) == 16)
-				cp_async16(dst, in + (bo | soff[r]));
+				cp_async16(dst, in + gi);
 			else
-				cp_async8(dst, in + (bo | soff[r]));
+				cp_async8(dst, in + gi);
 		}
 		cp_async_commit();
 	};
@@ -177,9 +213,11 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 			const dk_pass_desc *pd = passes + p;
 			const uint32_t sgb = nsgb, s0 = ns0, s1 = ns1, s2 = ns2;
 #pragma unroll
-			for (int r = 0; r < NA; ++r)
-				a[r] = tile[sgb ^ ((r & 1) ? s0 : 0u) ^ ((r & 2) ? s1 : 0u) ^
-					    ((r & 4) ? s2 : 0u)];
+			for (int r = 0; r < NA; ++r) {
+				const uint32_t sl = sgb ^ ((r & 1) ? s0 : 0u) ^ ((r & 2) ? s1 : 0u) ^
+						    ((r & 4) ? s2 : 0u);
+				a[r] = DK_IN_BOUNDS(sl, tn_amp, CHK_GATHER) ? tile[sl] : C2{};
+			}
 			if (p == 0) {
 #pragma unroll
 				for (int r = 0; r < NA; ++r)
@@ -208,9 +246,12 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 				apply_gate(a, pc, d.x & 0xffffu, d.y >> 16, d.z, d.w, smat + (d.x >> 16));
 			}
 #pragma unroll
-			for (int r = 0; r < NA; ++r)
-				tile[sgb ^ ((r & 1) ? s0 : 0u) ^ ((r & 2) ? s1 : 0u) ^
-				     ((r & 4) ? s2 : 0u)] = a[r];
+			for (int r = 0; r < NA; ++r) {
+				const uint32_t sl = sgb ^ ((r & 1) ? s0 : 0u) ^ ((r & 2) ? s1 : 0u) ^
+						    ((r & 4) ? s2 : 0u);
+				if (DK_IN_BOUNDS(sl, tn_amp, CHK_SCATTER))
+					tile[sl] = a[r];
+			}
 			/* the flag is uniform over the block */
 			if (pflags & DK_PASS_WARP)
 				__syncwarp();
@@ -218,8 +259,10 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 				__syncthreads();
 		}
 #pragma unroll
-		for (int r = 0; r < NA; ++r)
-			a[r] = tile[stid ^ sro[r]];
+		for (int r = 0; r < NA; ++r) {
+			const uint32_t so = stid ^ sro[r];
+			a[r] = DK_IN_BOUNDS(so, tn_amp, CHK_READOUT) ? tile[so] : C2{};
+		}
 		if (NBUF == 1) {
 			__syncthreads(); /* the buffer is free: start the next tile's copy */
 			tn = next_tile(t + gridDim.x);
@@ -230,7 +273,8 @@ __global__ void __launch_bounds__(1 << (M - DK_PASS_BITS), MINB)
 #pragma unroll
 		for (int r = 0; r < NA; ++r) {
 			outsq += sqabs(a[r]);
-			__stcs(out + (bo | soff[r]), a[r]);
+			if (DK_IN_BOUNDS(bo | soff[r], nglob, CHK_STORE))
+				__stcs(out + (bo | soff[r]), a[r]);
 		}
 		if (NBUF == 2)
 			__syncthreads(); /* this buffer is refilled two tiles later */
@@ -499,17 +543,23 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 		}
 		return ntiles;
 	};
+	[[maybe_unused]] const uint64_t nglob = 1ull << h->n;
 	auto prefetch = [&](uint64_t base, C2 *buf) {
 #pragma unroll
 		for (int h = 0; h < VT; ++h) {
 			const uint64_t bo = base | off_t(h);
 #pragma unroll
 			for (int r = 0; r < NA; ++r) {
-				C2 *dst = buf + (stid(h) ^ sro[r]);
+				const uint32_t so = stid(h) ^ sro[r];
+				const uint64_t gi = bo | soff[r];
+				if (!DK_IN_BOUNDS(so, tn_amp, CHK_LOAD_SMEM) ||
+				    !DK_IN_BOUNDS(gi, nglob, CHK_LOAD_GLOBAL))
+					continue;
+				C2 *dst = buf + so;
 				if (sizeof(C2) == 16)
-					cp_async16(dst, in + (bo | soff[r]));
+					cp_async16(dst, in + gi);
 				else
-					cp_async8(dst, in + (bo | soff[r]));
+					cp_async8(dst, in + gi);
 			}
 		}
 		cp_async_commit();
@@ -533,8 +583,11 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 #pragma unroll
 			for (int h = 0; h < VT; ++h)
 #pragma unroll
-				for (int r = 0; r < NA; ++r)
-					insq += sqabs(tile[stid(h) ^ sro[r]]);
+				for (int r = 0; r < NA; ++r) {
+					const uint32_t so = stid(h) ^ sro[r];
+					if (DK_IN_BOUNDS(so, tn_amp, CHK_READOUT))
+						insq += sqabs(tile[so]);
+				}
 			__syncthreads();
 		}
 		for (int p = 0; p < npass; ++p) {
@@ -572,8 +625,10 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 					const uint32_t sgl = sgl0 ^ __ldg(&pd->shi[warp + 8u * h]);
 					const uint32_t sgk = sgk0 ^ __ldg(&pn->shi[warp + 8u * h]);
 					const uint32_t bg = sgl ^ ((q & 1) ? t8 : 0u) ^ ((q & 2) ? t16 : 0u);
-					const C2 x0 = tile[bg ^ gj0];
-					const C2 x1 = tile[bg ^ gj1];
+					const C2 x0 = DK_IN_BOUNDS(bg ^ gj0, tn_amp, CHK_GATHER) ? tile[bg ^ gj0]
+												 : C2{};
+					const C2 x1 = DK_IN_BOUNDS(bg ^ gj1, tn_amp, CHK_GATHER) ? tile[bg ^ gj1]
+												 : C2{};
 					R y[4], z[4];
 					fa.product(x0, x1, y);
 					fb.load(mb);
@@ -584,7 +639,8 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 					for (int e = 0; e < 2; ++e) {
 						const uint32_t bs = sgk ^ (e ? u1 : 0u) ^ ((q & 1) ? u8 : 0u) ^
 								    ((q & 2) ? u16 : 0u);
-						tile[bs ^ sr] = c2_make<C2, R>(z[e], z[2 + e]);
+						if (DK_IN_BOUNDS(bs ^ sr, tn_amp, CHK_SCATTER))
+							tile[bs ^ sr] = c2_make<C2, R>(z[e], z[2 + e]);
 					}
 				}
 				__syncwarp();
@@ -627,8 +683,10 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 					const uint32_t shw = __ldg(&pd->shi[warp + 8u * h]);
 					const uint32_t sgl = sgl0 ^ shw, sgk = sgk0 ^ shw;
 					const uint32_t bg = sgl ^ ((q & 1) ? t8 : 0u) ^ ((q & 2) ? t16 : 0u);
-					const C2 x0 = tile[bg ^ gj0];
-					const C2 x1 = tile[bg ^ gj1];
+					const C2 x0 = DK_IN_BOUNDS(bg ^ gj0, tn_amp, CHK_GATHER) ? tile[bg ^ gj0]
+												 : C2{};
+					const C2 x1 = DK_IN_BOUNDS(bg ^ gj1, tn_amp, CHK_GATHER) ? tile[bg ^ gj1]
+												 : C2{};
 					R y[4];
 					fa.product(x0, x1, y);
 					__syncwarp(); /* the group's gathers precede its writes */
@@ -643,7 +701,8 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 						}
 						const uint32_t bs = sgk ^ (e ? t1 : 0u) ^ ((q & 1) ? t8 : 0u) ^
 								    ((q & 2) ? t16 : 0u);
-						tile[bs ^ sr] = c2_make<C2, R>(y[e], y[2 + e]);
+						if (DK_IN_BOUNDS(bs ^ sr, tn_amp, CHK_SCATTER))
+							tile[bs ^ sr] = c2_make<C2, R>(y[e], y[2 + e]);
 					}
 				}
 				__syncwarp();
@@ -654,8 +713,10 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 		if (VT == 1) {
 			C2 a[NA];
 #pragma unroll
-			for (int r = 0; r < NA; ++r)
-				a[r] = tile[stid(0) ^ sro[r]];
+			for (int r = 0; r < NA; ++r) {
+				const uint32_t so = stid(0) ^ sro[r];
+				a[r] = DK_IN_BOUNDS(so, tn_amp, CHK_READOUT) ? tile[so] : C2{};
+			}
 			__syncthreads(); /* the buffer is free */
 			tn = next_tile(t + gridDim.x);
 			if (tn < ntiles)
@@ -664,7 +725,8 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 #pragma unroll
 			for (int r = 0; r < NA; ++r) {
 				outsq += sqabs(a[r]);
-				__stcs(out + (bo | soff[r]), a[r]);
+				if (DK_IN_BOUNDS(bo | soff[r], nglob, CHK_STORE))
+					__stcs(out + (bo | soff[r]), a[r]);
 			}
 		} else {
 			/* two column sets: stream each amplitude out as it is read */
@@ -673,9 +735,11 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 				const uint64_t bo = base | off_t(h);
 #pragma unroll
 				for (int r = 0; r < NA; ++r) {
-					const C2 v = tile[stid(h) ^ sro[r]];
+					const uint32_t so = stid(h) ^ sro[r];
+					const C2 v = DK_IN_BOUNDS(so, tn_amp, CHK_READOUT) ? tile[so] : C2{};
 					outsq += sqabs(v);
-					__stcs(out + (bo | soff[r]), v);
+					if (DK_IN_BOUNDS(bo | soff[r], nglob, CHK_STORE))
+						__stcs(out + (bo | soff[r]), v);
 				}
 			}
 			__syncthreads(); /* the buffer is free */
@@ -953,7 +1017,7 @@ __global__ void __launch_bounds__(256)
 	for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < half;
 	     j += (uint64_t)gridDim.x * blockDim.x) {
 		const uint64_t i = ((j & ~low) << 1) | v | (j & low);
-		const C2 x = __ldcs(in + i);
+		const C2 x = DK_IN_BOUNDS(i, 2 * half, CHK_COLLAPSE) ? __ldcs(in + i) : C2{};
 		__stcs(out + j, x);
 		s += sqabs(x);
 	}
@@ -2229,3 +2293,27 @@ cudaError_t launch_copy(int prec, const void *src, void *dst, unsigned n,
 }
 
 } // namespace dk
+
+#ifdef DK_DEBUG_CHECKS
+/* Debug builds only: the first failed index check since the last reset, or 0
+ * (site in bits 56-63, index in bits 0-55); `reset` clears the record.  Call
+ * dk_sync() first so that every kernel has finished. */
+extern "C" int dk_debug_checks(uint64_t *first_failure, int reset)
+{
+	unsigned long long v = 0;
+	if (cudaMemcpyFromSymbol(&v, dk::g_dk_check, sizeof(v)) != cudaSuccess) {
+		cudaGetLastError();
+		return DK_ERR_CUDA;
+	}
+	if (reset) {
+		const unsigned long long zero = 0;
+		if (cudaMemcpyToSymbol(dk::g_dk_check, &zero, sizeof(zero)) != cudaSuccess) {
+			cudaGetLastError();
+			return DK_ERR_CUDA;
+		}
+	}
+	if (first_failure)
+		*first_failure = v;
+	return DK_OK;
+}
+#endif

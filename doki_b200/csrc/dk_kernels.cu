@@ -46,7 +46,8 @@ enum {
 	CHK_SCATTER = 4, /* tile slot written by a pass */
 	CHK_READOUT = 5, /* tile slot read for the write-back */
 	CHK_STORE = 6, /* amplitude index written to the register */
-	CHK_COLLAPSE = 7 /* amplitude index read by a collapse */
+	CHK_COLLAPSE = 7, /* amplitude index read by a collapse */
+	CHK_JOINT = 8 /* amplitude index read by a joint-distribution pass */
 };
 
 /* ---- fused sweep ------------------------------------------------------- */
@@ -1075,14 +1076,18 @@ __global__ void __launch_bounds__(256)
 	__syncthreads();
 	const uint64_t bin = blockIdx.y;
 	const uint64_t vb = deposit_mask(bin, mask);
+	[[maybe_unused]] const uint64_t nin = per_bin << __popcll(mask);
 	for (uint64_t c = blockIdx.x; c < nchunk; c += gridDim.x) {
 		double sum = 0.0, dummy = 0.0;
 		const uint64_t j0 = c * chunk;
 		uint64_t j1 = j0 + chunk;
 		if (j1 > per_bin)
 			j1 = per_bin;
-		for (uint64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x)
-			sum += sqabs(__ldcs(in + (dep_runs(sr, j) | vb)));
+		for (uint64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+			const uint64_t i = dep_runs(sr, j) | vb;
+			if (DK_IN_BOUNDS(i, nin, CHK_JOINT))
+				sum += sqabs(__ldcs(in + i));
+		}
 		block_sum2(dummy, sum);
 		if (threadIdx.x == 0)
 			partials[bin * nchunk + c] = sum;
@@ -1120,7 +1125,9 @@ __global__ void __launch_bounds__(256)
 		double p[16];
 #pragma unroll
 		for (int u = 0; u < 16; ++u)
-			p[u] = sqabs(__ldcs(in + base + t + 256u * u));
+			p[u] = DK_IN_BOUNDS(base + t + 256u * u, size, CHK_JOINT)
+				       ? sqabs(__ldcs(in + base + t + 256u * u))
+				       : 0.0;
 #pragma unroll
 		for (int u = 0; u < 16; ++u) {
 			const uint64_t i = base + t + 256u * u;
@@ -1208,7 +1215,8 @@ __global__ void k_decide_joint(const double *joint, int k, const double *rolls, 
 template <typename R>
 __global__ void __launch_bounds__(256)
 	k_collapse_joint(const typename CT<R>::T *__restrict__ in, typename CT<R>::T *out,
-			 DepRuns runs, uint64_t size, const uint64_t *vbits, double *partials)
+			 DepRuns runs, uint64_t size, const uint64_t *vbits, double *partials,
+			 [[maybe_unused]] uint64_t in_size)
 {
 	typedef typename CT<R>::T C2;
 	__shared__ DepRuns sr;
@@ -1219,7 +1227,8 @@ __global__ void __launch_bounds__(256)
 	double s = 0.0, dummy = 0.0;
 	for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < size;
 	     j += (uint64_t)gridDim.x * blockDim.x) {
-		const C2 x = __ldcs(in + (dep_runs(sr, j) | v));
+		const uint64_t i = dep_runs(sr, j) | v;
+		const C2 x = DK_IN_BOUNDS(i, in_size, CHK_COLLAPSE) ? __ldcs(in + i) : C2{};
 		__stcs(out + j, x);
 		s += sqabs(x);
 	}
@@ -2026,10 +2035,12 @@ cudaError_t launch_measure_joint(int prec, const void *in, void *out, unsigned n
 		const int blocks = grid_for(per_bin, 256 * 4, g_num_sms * 8);
 		if (prec == DK_C128)
 			k_collapse_joint<double><<<blocks, 256, 0, st>>>(
-				(const double2 *)in, (double2 *)out, runs, per_bin, vbits, s.partials);
+				(const double2 *)in, (double2 *)out, runs, per_bin, vbits, s.partials,
+				1ull << n);
 		else
 			k_collapse_joint<float><<<blocks, 256, 0, st>>>(
-				(const float2 *)in, (float2 *)out, runs, per_bin, vbits, s.partials);
+				(const float2 *)in, (float2 *)out, runs, per_bin, vbits, s.partials,
+				1ull << n);
 		k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc_in, sc_out, FIN_COLLAPSE, 1);
 		g_launches += 2;
 	}

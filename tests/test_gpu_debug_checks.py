@@ -1,13 +1,14 @@
 """The debug build (libdokigpu_dbg.so, -DDK_DEBUG_CHECKS) on the GPU.
 
-In that build the table-driven kernels -- both sweep kernels and the
-single-qubit collapse -- check every global and shared-memory index they
+In that build the table-driven kernels -- both sweep kernels, the
+joint-distribution passes and both collapses -- check every global and
+shared-memory index they
 compute; a failed check is recorded (site and index) and its access skipped,
 without a trap.  Seeded circuits run through the debug library's C ABI
 (tensor sweeps and, with DK_TENSOR=0, scalar sweeps; complex128 and
 complex64; gates with controls inside and outside the tile; joint
-measurement, and 13 qubits measured one at a time with the single-qubit
-collapse kernel).  No check may fire, and the results must equal
+measurement of 3, 4 and 6 qubits, and 13 qubits measured one at a time with
+the single-qubit collapse kernel).  No check may fire, and the results must equal
 the oracle's, as the release library's do.
 """
 from __future__ import annotations
@@ -123,6 +124,10 @@ def cases():
         "wide_c128": (wide, 2, (1 << 13) - 1, [0.66, 0.21, 0.45, 0.93, 0.12, 0.58, 0.37,
                                               0.81, 0.04, 0.49, 0.71, 0.26, 0.55], 13, 0.7),
         "wide_c64": (wide, 1, (1 << 17) | (1 << 9) | 1, [0.66, 0.21, 0.45], 13, 0.7),
+        # 6 measured qubits: the joint pass that gathers each outcome's
+        # amplitudes through the deposit tables (more than 4 bins)
+        "wide6_c128": (wide, 2, 0b10100100010010010, [0.5, 0.15, 0.85, 0.35, 0.62, 0.27], 3,
+                       0.2),
     }
 
 

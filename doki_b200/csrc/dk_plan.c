@@ -344,6 +344,44 @@ static int single_entry(const phase_ctx *cx, const dk_pass_desc *pd, uint32_t P)
 	return 1;
 }
 
+static const int perm3[6][3] = { { 0, 1, 2 }, { 0, 2, 1 }, { 1, 0, 2 },
+				 { 1, 2, 0 }, { 2, 0, 1 }, { 2, 1, 0 } };
+
+/* Fewest shared-memory wavefronts of a chained pair's gather (pass A) and
+ * scatter (pass B) over the orders of A's bits a and B's bits c (each in
+ * increasing order, permuted by perm3[*bo] and perm3[*bp]). */
+static int chain_orders(uint32_t PA, uint32_t PB, int m, int res, int *bo, int *bp)
+{
+	int a[3], c[3], na = 0, nc = 0;
+	for (int b = 0; b < m; b++) {
+		if (PA >> b & 1u)
+			a[na++] = b;
+		else if (PB >> b & 1u)
+			c[nc++] = b;
+	}
+	int best = 1 << 30;
+	*bo = *bp = 0;
+	for (int o = 0; o < 6; o++)
+		for (int q = 0; q < 6; q++) {
+			const int a0 = a[perm3[o][0]], a1 = a[perm3[o][1]], a2 = a[perm3[o][2]];
+			const int c0 = c[perm3[q][0]], c1 = c[perm3[q][1]], c2 = c[perm3[q][2]];
+			int cost;
+			if (res == 3) {
+				const int g[3] = { c0, a0, a1 }, t[3] = { c1, a1, a2 };
+				cost = (1 << (3 - nres(g, 3, 3))) + (1 << (3 - nres(t, 3, 3)));
+			} else {
+				const int g[4] = { c0, c1, a0, a1 }, t[4] = { c1, c2, a1, a2 };
+				cost = (1 << (4 - nres(g, 4, res))) + (1 << (4 - nres(t, 4, res)));
+			}
+			if (cost < best) {
+				best = cost;
+				*bo = o;
+				*bp = q;
+			}
+		}
+	return best;
+}
+
 /* Lane tables of a chained pair: pass A (bits a0 a1 a2, thread bits c0 c1
  * c2 r0 r1 W...) and pass B = (c1 c2 c0, thread bits a0 a1 a2 r0 r1 W...),
  * the orders picked for the fewest shared-memory wavefronts of A's gather
@@ -360,27 +398,9 @@ static void chain_pair(dk_pass_desc *pa, dk_pass_desc *pb, uint32_t PA, uint32_t
 		else if (!(W >> b & 1u) && nr < 2)
 			r[nr++] = b;
 	}
-	static const int perm[6][3] = { { 0, 1, 2 }, { 0, 2, 1 }, { 1, 0, 2 },
-					{ 1, 2, 0 }, { 2, 0, 1 }, { 2, 1, 0 } };
-	int best = 1 << 30, bo = 0, bp = 0;
-	for (int o = 0; o < 6; o++)
-		for (int q = 0; q < 6; q++) {
-			const int a0 = a[perm[o][0]], a1 = a[perm[o][1]], a2 = a[perm[o][2]];
-			const int c0 = c[perm[q][0]], c1 = c[perm[q][1]], c2 = c[perm[q][2]];
-			int cost;
-			if (res == 3) {
-				const int g[3] = { c0, a0, a1 }, t[3] = { c1, a1, a2 };
-				cost = (1 << (3 - nres(g, 3, 3))) + (1 << (3 - nres(t, 3, 3)));
-			} else {
-				const int g[4] = { c0, c1, a0, a1 }, t[4] = { c1, c2, a1, a2 };
-				cost = (1 << (4 - nres(g, 4, res))) + (1 << (4 - nres(t, 4, res)));
-			}
-			if (cost < best) {
-				best = cost;
-				bo = o;
-				bp = q;
-			}
-		}
+	const int(*perm)[3] = perm3;
+	int bo, bp;
+	chain_orders(PA, PB, m, res, &bo, &bp);
 	uint8_t laneA[32], laneB[32];
 	int nl = 0;
 	for (int j = 0; j < 3; j++) {
@@ -403,6 +423,46 @@ static void chain_pair(dk_pass_desc *pa, dk_pass_desc *pb, uint32_t PA, uint32_t
 	pass_tables_lanes(pb, pbB, laneB, nl, res);
 }
 
+/* Bits of a chained pair: A and B (disjoint target bits) each filled up to
+ * DK_PASS_BITS bits with disjoint fillers, chosen for the fewest
+ * shared-memory wavefronts of the pair (chain_orders), then for the fewest
+ * bits outside the phase's bits F (which may grow to fmax bits), then for
+ * the highest bits, as the plain fill takes them.  F holds at least
+ * 2 * DK_PASS_BITS bits, so a choice inside it always exists. */
+static void fill_pair(uint32_t A, uint32_t B, uint32_t F, int fmax, int m, int res,
+		      uint32_t *PA, uint32_t *PB)
+{
+	const uint32_t pool = ((1u << m) - 1u) & ~(A | B);
+	const int na = DK_PASS_BITS - popc(A), nb = DK_PASS_BITS - popc(B);
+	int best = 1 << 30;
+	*PA = A;
+	*PB = B;
+	/* submasks in decreasing order: the first of each size has the
+	 * highest bits */
+	for (uint32_t x = pool;; x = (x - 1) & pool) {
+		if (popc(x) == na) {
+			const uint32_t rest = pool & ~x;
+			for (uint32_t y = rest;; y = (y - 1) & rest) {
+				if (popc(y) == nb && popc(F | x | y) <= fmax) {
+					int bo, bp;
+					/* wavefronts first, then bits outside F */
+					const int c = 64 * chain_orders(A | x, B | y, m, res, &bo, &bp) +
+						      popc((x | y) & ~F);
+					if (c < best) {
+						best = c;
+						*PA = A | x;
+						*PB = B | y;
+					}
+				}
+				if (y == 0)
+					break;
+			}
+		}
+		if (x == 0)
+			break;
+	}
+}
+
 /* A phase: consecutive passes [0, cnt) whose pass bits all avoid the same
  * `wbits` tile bits W, which every pass maps to the thread bits above the 5
  * lane bits.  A warp then touches the same tile slots in every pass of the
@@ -413,10 +473,10 @@ static void chain_pair(dk_pass_desc *pa, dk_pass_desc *pb, uint32_t PA, uint32_t
  * Tensor sweeps: two neighbouring single-entry passes whose target bits are
  * disjoint chain in registers when their filled bit sets are disjoint too.
  * Such pairs are marked first (greedily from the front, which gives the most
- * pairs on a path) and filled from disjoint bits; the phase's union grows to
- * 2 * DK_PASS_BITS bits when it holds fewer, which still leaves the wbits
- * warp bits and the 2 lane bits a chained pair maps besides its 6 pass bits
- * (m - wbits = DK_PASS_BITS + 5). */
+ * pairs on a path) and filled from disjoint bits (fill_pair); the phase's
+ * union grows to at least 2 * DK_PASS_BITS and at most m - wbits bits, which
+ * still leaves the wbits warp bits and the 2 lane bits a chained pair maps
+ * besides its 6 pass bits (m - wbits = DK_PASS_BITS + 5). */
 static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, int wbits,
 			int res, int tensor, const phase_ctx *cx,
 			uint8_t (*pbits)[DK_PASS_BITS])
@@ -440,14 +500,12 @@ static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, 
 	}
 	for (int i = 0; i < cnt; i++) {
 		uint32_t P = need[i];
-		if (pair[i] || (i > 0 && pair[i - 1])) {
-			/* a chained pair: fillers avoid both passes' bits */
-			const int j = pair[i] ? i + 1 : i - 1;
-			const uint32_t avoid = need[j] | (pair[i] ? 0u : pmask[j]);
-			for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
-				if ((F & (1u << bit)) && !(avoid & (1u << bit)))
-					P |= 1u << bit;
+		if (pair[i]) {
+			fill_pair(need[i], need[i + 1], F, m - wbits, m, res, &P, &pmask[i + 1]);
+			F |= P | pmask[i + 1];
 		}
+		else if (i > 0 && pair[i - 1])
+			P = pmask[i]; /* filled with its partner */
 		for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
 			if (F & (1u << bit))
 				P |= 1u << bit;

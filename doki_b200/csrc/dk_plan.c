@@ -294,6 +294,41 @@ static int tc_best(uint32_t P, uint32_t L, int m, int res, uint8_t *pb, uint8_t 
 	return best;
 }
 
+/* The cost tc_best returns, without the choice: tc_cost depends on the lane
+ * bits only through their bank groups (bit % res), so the search runs over
+ * groups, each used at most as often as L has bits in it -- the same
+ * minimum over res^3 group triples instead of every ordered bit triple. */
+static int tc_best_cost(uint32_t P, uint32_t L, int m, int res)
+{
+	int p[DK_PASS_BITS], np = 0, cnt[4] = { 0, 0, 0, 0 }, best = 1 << 30;
+	for (int b = 0; b < m; b++) {
+		if (P >> b & 1u)
+			p[np++] = b;
+		else if (L >> b & 1u)
+			cnt[b % res]++;
+	}
+	static const int perm[6][3] = { { 0, 1, 2 }, { 0, 2, 1 }, { 1, 0, 2 },
+					{ 1, 2, 0 }, { 2, 0, 1 }, { 2, 1, 0 } };
+	for (int o = 0; o < 6; o++)
+		for (int x = 0; x < res; x++) {
+			if (cnt[x] < 1)
+				continue;
+			for (int y = 0; y < res; y++) {
+				if (cnt[y] < 1 + (y == x))
+					continue;
+				for (int z = 0; z < res; z++) {
+					if (cnt[z] < 1 + (z == x) + (z == y))
+						continue;
+					const int cost = tc_cost(p[perm[o][0]], p[perm[o][1]], x, y, z,
+								 res);
+					if (cost < best)
+						best = cost;
+				}
+			}
+		}
+	return best;
+}
+
 /* What build_phase needs to know about the gates of a sweep (tensor
  * sweeps) to decide which pairs of passes can chain in registers. */
 typedef struct phase_ctx {
@@ -527,8 +562,8 @@ static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, 
 				/* fewest shared-memory wavefronts of the tensor passes */
 				sc = 0;
 				for (int i = 0; i < cnt; i++)
-					sc -= tc_best(pmask[i], ((1u << m) - 1u) & ~pmask[i] & ~x, m,
-						      res, NULL, NULL);
+					sc -= tc_best_cost(pmask[i], ((1u << m) - 1u) & ~pmask[i] & ~x, m,
+							   res);
 			} else {
 				sc = phase_score(pmask, cnt, x, m, res);
 			}

@@ -248,14 +248,18 @@ static int nres(const int *b, int cnt, int res)
 	return popc(seen);
 }
 
+/* Wavefronts of a pass's gather and scatter per quarter-warp group, from the
+ * bank groups (bit % res) of pass bits 0, 1 and thread bits 0..2. */
 static int tc_cost(int pb0, int pb1, int l0, int l1, int l2, int res)
 {
 	if (res == 3) {
-		const int g[3] = { l0, pb0, pb1 }, t[3] = { pb0, l1, l2 };
-		return (1 << (3 - nres(g, 3, 3))) + (1 << (3 - nres(t, 3, 3)));
+		const int g = popc((1u << l0) | (1u << pb0) | (1u << pb1));
+		const int t = popc((1u << pb0) | (1u << l1) | (1u << l2));
+		return (1 << (3 - g)) + (1 << (3 - t));
 	}
-	const int g[4] = { l0, l1, pb0, pb1 }, t[4] = { pb0, pb1, l1, l2 };
-	return (1 << (4 - nres(g, 4, res))) + (1 << (4 - nres(t, 4, res)));
+	const int g = popc((1u << l0) | (1u << l1) | (1u << pb0) | (1u << pb1));
+	const int t = popc((1u << pb0) | (1u << pb1) | (1u << l1) | (1u << l2));
+	return (1 << (4 - g)) + (1 << (4 - t));
 }
 
 /* Cheapest order of pass bits P (register bits 0..2) and choice of thread
@@ -263,11 +267,15 @@ static int tc_cost(int pb0, int pb1, int l0, int l1, int l2, int res)
 static int tc_best(uint32_t P, uint32_t L, int m, int res, uint8_t *pb, uint8_t *l3)
 {
 	int p[DK_PASS_BITS], np = 0, l[32], nl = 0, best = 1 << 30;
+	int pr[DK_PASS_BITS], lr[32]; /* their bank groups */
 	for (int b = 0; b < m; b++) {
-		if (P >> b & 1u)
+		if (P >> b & 1u) {
+			pr[np] = b % res;
 			p[np++] = b;
-		else if (L >> b & 1u)
+		} else if (L >> b & 1u) {
+			lr[nl] = b % res;
 			l[nl++] = b;
+		}
 	}
 	static const int perm[6][3] = { { 0, 1, 2 }, { 0, 2, 1 }, { 1, 0, 2 },
 					{ 1, 2, 0 }, { 2, 0, 1 }, { 2, 1, 0 } };
@@ -277,8 +285,8 @@ static int tc_best(uint32_t P, uint32_t L, int m, int res, uint8_t *pb, uint8_t 
 				for (int c = 0; c < nl; c++) {
 					if (a == b2 || a == c || b2 == c)
 						continue;
-					const int cost = tc_cost(p[perm[o][0]], p[perm[o][1]], l[a],
-								 l[b2], l[c], res);
+					const int cost = tc_cost(pr[perm[o][0]], pr[perm[o][1]], lr[a],
+								 lr[b2], lr[c], res);
 					if (cost < best) {
 						best = cost;
 						if (pb)
@@ -303,7 +311,7 @@ static int tc_best_cost(uint32_t P, uint32_t L, int m, int res)
 	int p[DK_PASS_BITS], np = 0, cnt[4] = { 0, 0, 0, 0 }, best = 1 << 30;
 	for (int b = 0; b < m; b++) {
 		if (P >> b & 1u)
-			p[np++] = b;
+			p[np++] = b % res;
 		else if (L >> b & 1u)
 			cnt[b % res]++;
 	}

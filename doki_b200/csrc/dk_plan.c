@@ -546,9 +546,9 @@ static void build_phase(dk_pass_desc *pd, const uint32_t *need, int cnt, int m, 
 		if (pair[i]) {
 			fill_pair(need[i], need[i + 1], F, m - wbits, m, res, &P, &pmask[i + 1]);
 			F |= P | pmask[i + 1];
-		}
-		else if (i > 0 && pair[i - 1])
+		} else if (i > 0 && pair[i - 1]) {
 			P = pmask[i]; /* filled with its partner */
+		}
 		for (int bit = m - 1; popc(P) < DK_PASS_BITS && bit >= 0; bit--)
 			if (F & (1u << bit))
 				P |= 1u << bit;

@@ -238,10 +238,14 @@ class OracleDoki:
 
     def registry_measure(self, reg, mask, rolls, num_threads=-1, verbose=False):
         """doki.c:1023-1192: clone, then qubits n-1 .. 0 in mask, one roll each;
-        result[i] belongs to qubit n-1-i; returns (register or None, list)."""
+        result[i] belongs to qubit n-1-i; returns (register or None, list).
+        `last_margins` keeps |P(q=1) - roll| of each decision in measurement
+        order, so a checker can tell a rounding-level near-tie from a real
+        disagreement."""
         cur = self.registry_clone(reg)
         n0 = reg.n
         result = []
+        self.last_margins = []
         rid = 0
         measured = 0
         for i in range(n0):
@@ -256,6 +260,7 @@ class OracleDoki:
                 rid += 1
                 p1 = self.registry_prob(cur, q)
                 bit = p1 > roll
+                self.last_margins.append(abs(p1 - roll))
                 if cur.n == 1:
                     cur = OState(0, None, 0.0)
                 else:

@@ -26,6 +26,40 @@ ATOL_C128 = 1e-12
 ATOL_C64 = 5e-5
 
 
+# Near-tie tolerance of a measurement decision P(q=1) > roll: below it the
+# engine's rounding of P may legitimately flip the outcome.
+TIE_C128 = 1e-12
+TIE_C64 = 1e-6
+
+
+def assert_same_outcomes(got, want, margins, tol, where=""):
+    """Measurement outcomes of the engine (`got`) against the oracle's
+    (`want`), both in the reference's result layout (entry i for qubit
+    n-1-i; None or -1 = not measured).  `margins` are the oracle's
+    |P(q=1) - roll| per decision in measurement order.  Only the first
+    differing decision counts (later ones see another collapsed register):
+    with a margin below `tol` it is reported as a near-tie (xfail), otherwise
+    the comparison fails."""
+    def norm(v):
+        return None if v is None or (not isinstance(v, bool) and v == -1) else bool(v)
+
+    g, w = [norm(v) for v in got], [norm(v) for v in want]
+    assert len(g) == len(w), (g, w)
+    k = 0
+    for i, (gv, wv) in enumerate(zip(g, w)):
+        assert (gv is None) == (wv is None), f"measured qubits differ at entry {i}{where}"
+        if wv is None:
+            continue
+        if gv != wv:
+            margin = margins[k]
+            if margin < tol:
+                pytest.xfail(f"measurement near-tie{where}: entry {i}, |P - roll| = "
+                             f"{margin:.2e} < {tol:.0e}")
+            raise AssertionError(f"outcomes differ{where} at entry {i}: |P - roll| = "
+                                 f"{margin:.3e}, {g} != {w}")
+        k += 1
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
 

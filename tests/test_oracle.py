@@ -122,3 +122,30 @@ def test_oracle_vs_reference_random(orc, ref):
         assert np.allclose(va, orc.registry_get_all(b), atol=ATOL, rtol=0)
         pa = [ref.registry_prob(a, q, 1, False) for q in range(n)]
         assert np.allclose(pa, orc.registry_probs(b), atol=ATOL, rtol=0)
+
+
+def test_oracle_records_decision_margins(orc):
+    """registry_measure keeps |P(q=1) - roll| per decision; the first one is
+    the top measured qubit's marginal against the first roll."""
+    c = W.small_circuit(seed=5, n=8, depth=3)
+    reg = W.run_ops(orc, orc.registry_new(8), c.ops)
+    p_top = orc.registry_prob(reg, 7)
+    rolls = [0.41, 0.62, 0.17]
+    orc.registry_measure(reg, 0b10000011, rolls)
+    assert len(orc.last_margins) == 3
+    assert orc.last_margins[0] == pytest.approx(abs(p_top - rolls[0]), abs=1e-15)
+
+
+def test_outcome_check_reports_near_ties_only():
+    from tests.conftest import assert_same_outcomes
+    same = [1, -1, 0]
+    assert_same_outcomes(same, [True, None, False], [0.3, 0.2], 1e-12)
+    # the first differing decision is within rounding of its roll: near-tie
+    with pytest.raises(pytest.xfail.Exception):
+        assert_same_outcomes([1, -1, 1], [True, None, False], [0.3, 5e-14], 1e-12)
+    # a clear disagreement fails, even when a later margin is tiny
+    with pytest.raises(AssertionError):
+        assert_same_outcomes([0, -1, 1], [True, None, False], [0.3, 5e-14], 1e-12)
+    # different measured sets fail
+    with pytest.raises(AssertionError):
+        assert_same_outcomes([1, 0, 0], [True, None, False], [0.3, 0.2], 1e-12)

@@ -16,6 +16,8 @@ metric: gate-layers per second (40 per step), whole job over all GPUs.
 --gpus N runs N independent replicas (the path does not shard at this size).
 --impl reference times the reference Doki CPU module (compiled from source
 into oracle/_ref) on the host cores, one workload gate per step.
+The line also carries `per_gate`: the same register with fusion off (one
+sweep per gate, the plain per-gate method) against the HBM roofline.
 """
 from __future__ import annotations
 
@@ -164,10 +166,12 @@ def job_rate(world, units_per_rank, seconds):
     return world * units_per_rank / seconds
 
 
-def run_job(d, c, gates, keep, rolls_mask, rolls, prec="c128"):
-    """One full workload through the public API; returns the host results."""
+def run_job(d, c, gates, keep, rolls_mask, rolls, prec="c128", reg=None):
+    """The workload's gates queued through the public API on a new |0..0>
+    register (or on `reg`); returns the register (gates not yet flushed)."""
     n = c.num_qubits
-    reg = d.registry_new(n, False) if prec == "c128" else d.registry_new(n, False, 1)
+    if reg is None:
+        reg = d.registry_new(n, False) if prec == "c128" else d.registry_new(n, False, 1)
     for op, g in zip(c.ops, gates):
         ctl = set(op.controls) if (op.controls or op.anticontrols) else None
         reg = d.registry_apply(reg, g, list(op.targets), ctl, set(op.anticontrols) or None,
@@ -204,6 +208,52 @@ def tensor_roofline(entry_amps, sweep_s, c64, clk, steps):
         out.update({"peak": peak, "frac": achieved / peak,
                     "peak_kind": f"ncu FP64 MMA op rate 128/SM/cycle x {sms} SMs x {mhz:g} MHz"})
     return out
+
+
+def per_gate_record(d, c, prec, torch, stream, layers=2):
+    """The plain per-gate method on the benchmark register: fusion off, so
+    every gate of the first `layers` layers is its own in-place sweep over
+    the whole register (the reference's one loop per apply_gate,
+    qops.c:211-257).  Algorithmic bytes per gate: 2 S 2^-c for c controls
+    and anticontrols (amplitudes whose conditions fail need not move);
+    achieved = their sum / the sweeps' device time."""
+    n = c.num_qubits
+    ops = c.ops[:c.layer_starts[layers]]
+    state_bytes = (8 if prec == "c64" else 16) << n
+    gates = [d.gate_new(op.k, op.gate.tolist(), False) for op in ops]
+    reg = d.registry_new(n, False) if prec == "c128" else d.registry_new(n, False, 1)
+    d.registry_flush(reg)
+    d.engine_set_fusion(False)
+    try:
+        reg = run_job(d, W_ops(c, ops), gates, 0, 0, [], prec, reg=reg)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0 = d.engine_stats()["sweeps"]
+        e0.record(stream)
+        d.registry_flush(reg)
+        e1.record(stream)
+        e1.synchronize()
+        sweeps = d.engine_stats()["sweeps"] - s0
+    finally:
+        d.engine_set_fusion(True)
+    del reg
+    ms = e0.elapsed_time(e1)
+    algo = sum(2 * state_bytes >> (len(op.controls) + len(op.anticontrols)) for op in ops)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = algo / (ms / 1e3) / 1e9
+    return {"gates": len(ops), "layers": layers, "sweeps": sweeps, "device_ms": ms,
+            "avg_sweep_ms": ms / max(1, sweeps),
+            "kernel": "one in-place fused-sweep launch per gate (fusion off)",
+            "algorithmic_bytes": algo, "achieved": achieved, "unit": "GB/s", "peak": peak,
+            "peak_kind": peak_kind + " hbm_gbs (copy)", "frac": achieved / peak,
+            "gate_layers_per_s": layers / (ms / 1e3)}
+
+
+class W_ops:
+    """A circuit restricted to a list of its ops (for run_job)."""
+
+    def __init__(self, c, ops):
+        self.num_qubits = c.num_qubits
+        self.ops = ops
 
 
 def engine_arm(args, rank, world, local_rank):
@@ -323,6 +373,8 @@ def engine_arm(args, rank, world, local_rank):
         "clocks": clk,
         "fusion": not args.no_fusion,
     }
+    if rank == 0 and world == 1:
+        out["per_gate"] = per_gate_record(d, c, args.precision, torch, stream)
     if rank == 0 and world == 1 and not args.no_forms:
         out["forms"] = run_forms(d, args, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -426,8 +478,12 @@ def precision_form(d):
     r = P.run(d, n=32, depth=60, seed=1)
     return {"workload": "32-qubit register, complex64 (32 GiB) beside complex128 (64 GiB), "
                         "depth-60 circuit of the 12-qubit generator family",
-            "worst": r["worst"], "c64_layers_per_s": r["c64_layers_per_s"],
-            "c128_layers_per_s": r["c128_layers_per_s"],
+            "worst": r["worst"],
+            "c64_layers_per_s_flushed_each_layer": r["c64_layers_per_s_flushed_each_layer"],
+            "c128_layers_per_s_flushed_each_layer": r["c128_layers_per_s_flushed_each_layer"],
+            "c64_layers_per_s_fused": r["c64_layers_per_s_fused"],
+            "c128_layers_per_s_fused": r["c128_layers_per_s_fused"],
+            "fused_final": r["fused_final"],
             "fidelity_per_layer": [round(x["fidelity"], 12) for x in r["layers"]]}
 
 
@@ -446,54 +502,114 @@ def run_forms(d, args, torch):
 
 # --------------------------------------------------------------- reference --
 
-def sample_ops(c):
-    """Gates of the first layer, spread over low / high qubits and 2-qubit ops."""
-    layer = c.ops[c.layer_starts[0]:c.layer_starts[1]]
-    idx = [0, len(layer) // 2 - 1, len(layer) - 1, 7, len(layer) // 2 + 3, 15]
-    return [layer[i % len(layer)] for i in idx]
+def layer_ops(c, layer=0):
+    return c.ops[c.layer_starts[layer]:c.layer_starts[layer + 1]]
 
 
-def reference_timings(n, c, count, warm=0):
+def gate_kind(op):
+    """"cond": a gate the generator gave extra controls / anticontrols;
+    "pair": a brickwork CZ / CNOT (one control); "u3": an uncontrolled U3."""
+    if op.anticontrols or len(op.controls) > 1:
+        return "cond"
+    if op.controls:
+        return "pair" if abs(op.gate[0, 0]) in (0.0, 1.0) else "cond"
+    return "u3"
+
+
+def stratified_order(ops):
+    """Indices of a layer's gates in an order whose every prefix mixes the
+    kinds: the conditioned gates first, then pairs and U3s alternating."""
+    by = {"cond": [], "pair": [], "u3": []}
+    for i, op in enumerate(ops):
+        by[gate_kind(op)].append(i)
+    order = list(by["cond"])
+    pairs, u3s = by["pair"], by["u3"]
+    for j in range(max(len(pairs), len(u3s))):
+        order += pairs[j:j + 1] + u3s[j:j + 1]
+    return order
+
+
+def ref_apply(ref, reg, op, threads):
+    g = ref.gate_new(op.k, op.gate.tolist(), False)
+    ctl = set(op.controls) if (op.controls or op.anticontrols) else None
+    return ref.registry_apply(reg, g, list(op.targets), ctl, set(op.anticontrols) or None,
+                              threads, False)
+
+
+def reference_layer(n, c, threads):
+    """One full layer of the workload through the reference module (all its
+    gates in order, conditioned ones included), then registry_prob of one
+    qubit and a one-qubit registry_measure (clone + probability + collapse,
+    doki.c:1023-1192), each timed around the Python call as the reference's
+    tests/timed_test.py:11-44 does."""
     from oracle import oracle as O
-    from doki_b200 import workloads as W
     ref = O.reference_module()
-    threads = os.cpu_count() or 1
-    ops = sample_ops(c)
+    ops = layer_ops(c)
     reg = ref.registry_new(n, False)
-    times = []
-    for i in range(warm + count):
-        op = ops[i % len(ops)]
-        g = ref.gate_new(op.k, op.gate.tolist(), False)
-        ctl = set(op.controls) if (op.controls or op.anticontrols) else None
-        t0 = time.perf_counter()
-        new = ref.registry_apply(reg, g, list(op.targets), ctl,
-                                 set(op.anticontrols) or None, threads, False)
-        dt = time.perf_counter() - t0
-        del reg
-        reg = new
-        if i >= warm:
-            times.append(dt)
-    del reg
-    return times, threads
+    t0 = time.perf_counter()
+    for op in ops:
+        reg = ref_apply(ref, reg, op, threads)
+    t_layer = time.perf_counter() - t0
+    q = max(q for q in range(n) if (c.measure_mask >> q) & 1)
+    t0 = time.perf_counter()
+    ref.registry_prob(reg, q, threads, False)
+    t_prob = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sub, _ = ref.registry_measure(reg, 1 << q, [float(c.rolls[0])], threads, False)
+    t_meas = time.perf_counter() - t0
+    del sub, reg
+    return {"gates": len(ops), "layer_s": t_layer, "prob_s": t_prob, "measure1_s": t_meas}
+
+
+def reference_one_gate(n, c, threads):
+    """One U3 of the workload on the reference module with `threads` threads."""
+    from oracle import oracle as O
+    ref = O.reference_module()
+    op = next(op for op in layer_ops(c) if gate_kind(op) == "u3")
+    reg = ref.registry_new(n, False)
+    t0 = time.perf_counter()
+    new = ref_apply(ref, reg, op, threads)
+    dt = time.perf_counter() - t0
+    del new, reg
+    return dt
 
 
 def cpu_baseline(n, c):
-    gates_per_layer = len(c.ops) / c.depth
+    """The reference CPU path on the box's host cores: one measured full
+    layer of the 30-qubit workload at all threads (plus one probability and
+    one single-qubit measurement), and one U3 at a single thread.  The job's
+    layers/s is depth / (depth x layer + n x prob + 4 x one-qubit measure);
+    the 30 -> 10-qubit reduced density matrix, which the reference's lazy
+    functional matrices cannot evaluate in any useful time
+    (funmatrix.c:920-944: 2^20 recursive leaves per element), is left out."""
+    threads = os.cpu_count() or 1
     try:
-        times, threads = reference_timings(n, c, 4)
-        qn = n
+        lay = reference_layer(n, c, threads)
+        one = reference_one_gate(n, c, 1)
     except MemoryError:
-        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
                 "sample": "host memory too small for the reference at this size"}
-    per_gate = statistics.mean(times)
-    return {"value": 1.0 / (per_gate * gates_per_layer), "unit": UNIT, "cores": threads,
-            "kind": "reference",
-            "sample": (f"reference doki registry_apply (OpenMP, {threads} threads) on {qn} "
-                       f"qubits: {len(times)} gates from layer 0 (low/high U3, CNOT/CZ), "
-                       f"mean {per_gate:.3f} s/gate x {gates_per_layer:.1f} gates/layer")}
+    nmeas = bin(c.measure_mask).count("1")
+    job_s = c.depth * lay["layer_s"] + n * lay["prob_s"] + nmeas * lay["measure1_s"]
+    return {"value": c.depth / job_s, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": (f"reference doki module (compiled from its sources, OpenMP, {threads} "
+                       f"threads) on the {n}-qubit register: layer 0 of the workload measured "
+                       f"whole ({lay['gates']} gates incl. the conditioned ones) in "
+                       f"{lay['layer_s']:.1f} s, registry_prob {lay['prob_s']:.2f} s, 1-qubit "
+                       f"registry_measure {lay['measure1_s']:.2f} s; job = {c.depth} layers + "
+                       f"{n} probabilities + {nmeas} one-qubit measurements"),
+            "layer": lay, "one_thread": {"cores": 1, "u3_gate_s": one,
+                                         "gate_layers_per_s_est":
+                                             1.0 / (one * len(layer_ops(c)))}}
 
 
 def reference_arm(args, rank, world):
+    """The reference's own CPU implementation of the path on the host cores,
+    one workload gate per step.  The steps walk the 30-qubit workload's first
+    layer in an order that mixes its gate kinds from the start (conditioned
+    gates, then CZ / CNOT pairs and U3s alternating); layers/s is estimated
+    per kind: 1 / sum over kinds of (gates of that kind per layer x mean
+    measured seconds per gate of that kind)."""
     if rank != 0:
         return
     from doki_b200 import workloads as W
@@ -504,16 +620,40 @@ def reference_arm(args, rank, world):
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference module not built (oracle/_ref)"}))
         return
-    times, threads = reference_timings(n, c, args.steps, warm=args.warmup)
-    gates_per_layer = len(c.ops) / c.depth
-    per_gate = statistics.mean(times)
-    value = 1.0 / (per_gate * gates_per_layer)
-    sample = (f"one workload gate per step on {n} qubits (layer-0 U3 low/high, CNOT/CZ), "
-              f"layers/s = 1 / (mean s/gate x {gates_per_layer:.1f} gates/layer)")
+    ref = O.reference_module()
+    threads = os.cpu_count() or 1
+    ops = layer_ops(c)
+    order = stratified_order(ops)
+    L = len(order)
+    reg = ref.registry_new(n, False)
+    for j in range(args.warmup):
+        reg = ref_apply(ref, reg, ops[order[(L - args.warmup + j) % L]], threads)
+    times = {"cond": [], "pair": [], "u3": []}
+    all_t = []
+    for k in range(args.steps):
+        op = ops[order[k % L]]
+        t0 = time.perf_counter()
+        new = ref_apply(ref, reg, op, threads)
+        dt = time.perf_counter() - t0
+        reg = new
+        times[gate_kind(op)].append(dt)
+        all_t.append(dt)
+    del reg
+    mean_all = statistics.mean(all_t)
+    counts = {kd: sum(1 for op in ops if gate_kind(op) == kd) for kd in times}
+    layer_s = sum(counts[kd] * (statistics.mean(v) if v else mean_all)
+                  for kd, v in times.items())
+    per_layer = len(c.ops) / c.depth
+    layer_s *= per_layer / len(ops)  # layers of the workload average per_layer gates
+    value = 1.0 / layer_s
+    sample = (f"one gate per step on {n} qubits, walking layer 0's {len(ops)} gates "
+              f"({counts['cond']} conditioned, {counts['pair']} CZ/CNOT, {counts['u3']} U3) "
+              f"in a kind-mixing order; layers/s = 1 / sum over kinds of gates per layer x "
+              f"mean measured s/gate ({ {k: len(v) for k, v in times.items()} } samples)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": per_gate * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": mean_all * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(n, depth, c),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",

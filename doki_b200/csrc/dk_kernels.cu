@@ -1667,7 +1667,7 @@ int g_num_sms = 148;
 
 } // namespace
 
-unsigned long long g_launches = 0;
+std::atomic<unsigned long long> g_launches{0};
 
 /* ---------------------------------------------------------------------- */
 
@@ -1932,10 +1932,31 @@ cudaError_t launch_marginals_blocks(int prec, const void *d, unsigned n,
 		threads = 32;
 		sbits = (int)n;
 	}
-	launch_marginals_kernel(prec, d, n, sbits, blocks, threads, s.partials, st);
-	k_marg_finalize<<<1, 64, 0, st>>>(s.partials, blocks, (int)n, s.marg);
-	g_launches += 2;
-	return cudaGetLastError();
+	/* cudaLaunchKernel returns the status of this launch alone: an error
+	 * left pending by the caller's earlier, unrelated work is neither
+	 * reported as this call's failure nor cleared */
+	const int nb = (int)n - sbits;
+	const void *kern;
+	if (prec == DK_C128)
+		kern = nb <= 12 ? (const void *)k_marginals<double, 12>
+		       : nb <= 16 ? (const void *)k_marginals<double, 16>
+				  : (const void *)k_marginals<double, kMargHi>;
+	else
+		kern = nb <= 12 ? (const void *)k_marginals<float, 12>
+		       : nb <= 16 ? (const void *)k_marginals<float, 16>
+				  : (const void *)k_marginals<float, kMargHi>;
+	const void *amps = d;
+	int ni = (int)n, sb = sbits;
+	double *partials = s.partials, *marg = s.marg;
+	void *kargs[] = { (void *)&amps, (void *)&ni, (void *)&sb, (void *)&partials };
+	cudaError_t e = cudaLaunchKernel(kern, dim3(blocks), dim3(threads), kargs, 0, st);
+	if (e != cudaSuccess)
+		return e;
+	int nblk = blocks;
+	void *fargs[] = { (void *)&partials, (void *)&nblk, (void *)&ni, (void *)&marg };
+	e = cudaLaunchKernel((const void *)k_marg_finalize, dim3(1), dim3(64), fargs, 0, st);
+	g_launches += (e == cudaSuccess) ? 2 : 1;
+	return e;
 }
 
 cudaError_t launch_measure_collapse(int prec, const void *in, void *out,

@@ -5,12 +5,16 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "dk_internal.h"
 
 namespace dk {
 
-/* Kernels launched by the wrappers below (for the engine's counters). */
-extern unsigned long long g_launches;
+/* Kernels launched by the wrappers below (for the engine's counters).
+ * Several slot threads launch at once, so the count is atomic: it orders
+ * nothing, it only must not lose increments. */
+extern std::atomic<unsigned long long> g_launches;
 
 /* Number of per-block partial slots the scratch buffer must hold. */
 constexpr int kMaxBlocks = 4096;

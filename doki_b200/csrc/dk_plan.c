@@ -1398,7 +1398,19 @@ int dk_plan_build(const dk_flat_op *ops, int nops, unsigned n, int prec,
 			nrem--;
 			continue;
 		}
-		/* complete Q to m bits with the lowest free qubits */
+		/* complete Q to m bits with the lowest free qubits.  One gate per
+		 * sweep (no fusion): leave its controls and anticontrols out of the
+		 * tile where the register has room, so that they become tile
+		 * conditions and an in-place sweep skips the tiles where they fail
+		 * (2 S 2^-c bytes moved for c such qubits instead of 2 S). */
+		if (!lim->fuse && nt == 1) {
+			const dk_flat_op *op = &ops[take[0]];
+			const uint64_t cond = (op->cm | op->am) & ~Q;
+			if ((unsigned)popc(cond) <= n - (unsigned)m)
+				for (unsigned q = 0; popc(Q) < m && q < n; q++)
+					if (!((cond >> q) & 1u))
+						Q |= UINT64_C(1) << q;
+		}
 		for (unsigned q = 0; popc(Q) < m && q < n; q++)
 			Q |= UINT64_C(1) << q;
 		if (emit_sweep(&b, ops, take, nt, Q, n, prec, m, kinds, &fold,

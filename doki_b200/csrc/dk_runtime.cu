@@ -1186,6 +1186,65 @@ int dk_measure(dk_state *s, unsigned target, double roll, int *result,
 	return DK_OK;
 }
 
+namespace {
+
+/* The join itself, on most's slot (locked by the caller).  `ready`: an event
+ * on least's stream that most's stream must wait for first (least was
+ * flushed on its own slot), or NULL.  On success with a cross-slot join,
+ * *done is an event recorded on most's stream after the join kernel. */
+int join_on_most(dk_state *most, dk_state *least, cudaEvent_t ready, dk_state **out,
+		 cudaEvent_t *done)
+{
+	int rc = prepare_read(most);
+	if (rc == DK_OK && !ready)
+		rc = prepare_read(least);
+	if (ready && rc == DK_OK && cudaStreamWaitEvent(CUR.st, ready, 0) != cudaSuccess)
+		rc = cuda_fail(cudaGetLastError());
+	if (rc)
+		return rc;
+	if (!out || most->prec != least->prec)
+		return DK_ERR_ARG;
+	const unsigned n = most->n + least->n;
+	if (n > DK_MAX_QUBITS)
+		return DK_ERR_QUBITS;
+	dk_state *s = state_alloc(n, most->prec, most->slot);
+	if (!s)
+		return DK_ERR_ALLOC;
+	rc = buf_new(n, most->prec, &s->buf);
+	if (rc) {
+		free(s);
+		return rc;
+	}
+	cudaError_t e = dk::launch_join(most->prec, most->buf->d, most->n, most->buf->sc,
+					least->buf->d, least->n, least->buf->sc,
+					s->buf->d, s->buf->sc, CUR.scratch, CUR.st);
+	if (e == cudaSuccess && ready) {
+		cudaEvent_t ev = nullptr;
+		e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+		if (e == cudaSuccess) {
+			e = cudaEventRecord(ev, CUR.st);
+			if (e == cudaSuccess)
+				*done = ev;
+			else
+				cudaEventDestroy(ev);
+		}
+		if (e != cudaSuccess) {
+			/* no event to order least's stream by: the join kernel is
+			 * queued, so wait for it here instead */
+			cudaGetLastError();
+			e = cudaStreamSynchronize(CUR.st);
+		}
+	}
+	if (e != cudaSuccess) {
+		dk_state_free(s);
+		return cuda_fail(e);
+	}
+	*out = s;
+	return DK_OK;
+}
+
+} // namespace
+
 int dk_join(dk_state *most, dk_state *least, dk_state **out)
 {
 	DK_TRACE();
@@ -1206,39 +1265,30 @@ int dk_join(dk_state *most, dk_state *least, dk_state **out)
 			return cuda_fail(cudaGetLastError());
 		}
 	}
-	SlotLock lk(most->slot);
-	rc = prepare_read(most);
-	if (rc == DK_OK && !ready)
-		rc = prepare_read(least);
-	if (ready) {
-		if (rc == DK_OK && cudaStreamWaitEvent(CUR.st, ready, 0) != cudaSuccess)
-			rc = cuda_fail(cudaGetLastError());
+	cudaEvent_t done = nullptr;
+	{
+		SlotLock lk(most->slot);
+		rc = join_on_most(most, least, ready, out, &done);
+	}
+	if (ready)
 		cudaEventDestroy(ready);
+	if (done) {
+		/* The join kernel reads least's buffer on most's stream.  Whatever
+		 * least's slot queues next (freeing that buffer on its stream, or
+		 * overwriting it in place when a register derived from least is
+		 * flushed) waits for that read.  The two slot locks are taken one
+		 * after the other, never nested, so joins in opposite directions
+		 * cannot deadlock. */
+		SlotLock lk2(least->slot);
+		if (cudaStreamWaitEvent(CUR.st, done, 0) != cudaSuccess) {
+			/* not ordered: wait for the join itself instead */
+			cudaGetLastError();
+			if (cudaEventSynchronize(done) != cudaSuccess && rc == DK_OK)
+				rc = cuda_fail(cudaGetLastError());
+		}
+		cudaEventDestroy(done);
 	}
-	if (rc)
-		return rc;
-	if (!out || most->prec != least->prec)
-		return DK_ERR_ARG;
-	const unsigned n = most->n + least->n;
-	if (n > DK_MAX_QUBITS)
-		return DK_ERR_QUBITS;
-	dk_state *s = state_alloc(n, most->prec, most->slot);
-	if (!s)
-		return DK_ERR_ALLOC;
-	rc = buf_new(n, most->prec, &s->buf);
-	if (rc) {
-		free(s);
-		return rc;
-	}
-	cudaError_t e = dk::launch_join(most->prec, most->buf->d, most->n, most->buf->sc,
-					least->buf->d, least->n, least->buf->sc,
-					s->buf->d, s->buf->sc, CUR.scratch, CUR.st);
-	if (e != cudaSuccess) {
-		dk_state_free(s);
-		return cuda_fail(e);
-	}
-	*out = s;
-	return DK_OK;
+	return rc;
 }
 
 int dk_reduced_density(dk_state *s, uint64_t keep_mask, double *out)

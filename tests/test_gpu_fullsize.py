@@ -1,8 +1,11 @@
-"""Full-size checks at 30 qubits (16 GiB complex128 registers), where the
-oracle is too slow to run: the sizes of the benchmark workload, with the
-global qubits 26-29 that the oracle-parity tests (26 qubits and below) never
-touch.  Each test checks a property that holds exactly for any correct
-state-vector engine, to the complex128 tolerance of the parity tests:
+"""Full-size checks at 30 qubits (16 GiB complex128 registers), where a
+whole-circuit oracle run is too slow: the sizes of the benchmark workload,
+with the qubits 26-29 that the oracle-parity tests (26 qubits and below,
+``test_gpu_config2.py`` and ``test_gpu_parity.py``) never reach; the one
+30-qubit comparison with the reference itself is the benchmark's first
+layer (``test_gpu_config2.py``).  Each test here checks a property that holds
+exactly for any correct state-vector engine, to the complex128 tolerance of
+the parity tests:
 
 - a product state after permutation and phase gates against its closed form,
   amplitude by amplitude at sampled indices (reference qops.c:176-261);

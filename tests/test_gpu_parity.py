@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 from doki_b200 import workloads as W
-from tests.conftest import ATOL_C128, ATOL_C64, TIE_C128, TIE_C64, assert_same_outcomes
+from tests.conftest import (ATOL_C128, ATOL_C64, TIE_C128, TIE_C64, NearTies,
+                            assert_same_outcomes)
 from tests.golden.gen_golden import random_unitary
 from tests.test_plan import random_ops
 
@@ -252,15 +253,18 @@ def test_measure_sequence_vs_oracle(dk_gpu, orc):
     a = W.run_ops(d, d.registry_new(n, False), ops)
     b = W.run_ops(orc, orc.registry_new(n), ops)
     rng = W.rng_for(32)
+    ties = NearTies()
     for trial in range(6):
         mask = int(rng.integers(1, 1 << n))
         rolls = rng.random(bin(mask).count("1")).tolist()
         ra, resa = d.registry_measure(a, mask, rolls, 1, False)
         rb, resb = orc.registry_measure(b, mask, rolls)
-        assert_same_outcomes(res_list(resa), res_list(resb), orc.last_margins, TIE_C128,
-                             f" (trial {trial})")
+        if not ties.check(res_list(resa), res_list(resb), orc.last_margins, TIE_C128,
+                          f" (trial {trial})"):
+            continue
         if rb is not None:
             assert np.allclose(allamps(d, ra), orc.registry_get_all(rb), atol=ATOL_C128, rtol=0)
+    ties.finish()
 
 
 @pytest.mark.parametrize("n,prec", [(22, 2), (20, 1), (13, 2)])
@@ -280,16 +284,19 @@ def test_measure_joint_vs_oracle(dk_gpu, orc, n, prec):
              sum(1 << int(q) for q in rng.choice(n, size=5, replace=False)),
              sum(1 << int(q) for q in rng.choice(n, size=6, replace=False)),
              0b1111111]
+    ties = NearTies()
     for mask in masks:
         for _ in range(3):
             rolls = rng.random(bin(mask).count("1")).tolist()
             ra, resa = d.registry_measure(a, mask, rolls, 1, False)
             rb, resb = orc.registry_measure(b, mask, rolls)
-            assert_same_outcomes(res_list(resa), res_list(resb), orc.last_margins,
-                                 TIE_C128 if prec == 2 else TIE_C64, f" (mask {mask:#x})")
+            if not ties.check(res_list(resa), res_list(resb), orc.last_margins,
+                              TIE_C128 if prec == 2 else TIE_C64, f" (mask {mask:#x})"):
+                continue
             if rb is not None:
                 tol = ATOL_C128 if prec == 2 else ATOL_C64
                 assert np.allclose(allamps(d, ra), orc.registry_get_all(rb), atol=tol, rtol=0)
+    ties.finish()
 
 
 def test_measure_joint_unnormalised_data(dk_gpu, orc):
@@ -301,16 +308,19 @@ def test_measure_joint_unnormalised_data(dk_gpu, orc):
     vals = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)) * 0.07
     a = d.registry_new_data(n, vals.tolist(), False)
     b = orc.registry_new_data(n, vals.tolist())
+    ties = NearTies()
     for mask in (0b101, 0b110000001, (1 << n) - 1):
         for _ in range(4):
             rolls = rng.random(bin(mask).count("1")).tolist()
             ra, resa = d.registry_measure(a, mask, rolls, 1, False)
             rb, resb = orc.registry_measure(b, mask, rolls)
-            assert_same_outcomes(res_list(resa), res_list(resb), orc.last_margins, TIE_C128,
-                                 f" (mask {mask:#x})")
+            if not ties.check(res_list(resa), res_list(resb), orc.last_margins, TIE_C128,
+                              f" (mask {mask:#x})"):
+                continue
             if rb is not None:
                 assert np.allclose(allamps(d, ra), orc.registry_get_all(rb), atol=ATOL_C128,
                                    rtol=0)
+    ties.finish()
 
 
 def test_reduced_density_vs_oracle(dk_gpu, orc, oracle_mod):
@@ -538,3 +548,26 @@ def test_tensor_work_counter(dk_gpu):
     d.registry_flush(r)
     grown = d.engine_stats()["mma_entry_amplitudes"] - before
     assert grown > 0 and grown % (1 << n) == 0
+
+
+def test_registry_mem_reports_device_storage(dk_gpu):
+    """registry_mem (reference state_mem_size, qstate.c:123-135: header +
+    amplitude storage) reports the register's device amplitude bytes
+    (16 or 8 per amplitude) plus a fixed part -- the host header and the
+    device scalar block -- that does not depend on the size.  A clone shares
+    the storage and reports the same; a deleted registry reports the fixed
+    host header only."""
+    d = dk_gpu
+    fixed = set()
+    for n in (1, 5, 12, 20):
+        for prec, amp in ((2, 16), (1, 8)):
+            r = d.registry_new(n, False, prec)
+            fixed.add(d.registry_mem(r, False) - (amp << n))
+            c = d.registry_clone(r, 1, False)
+            assert d.registry_mem(c, False) == d.registry_mem(r, False)
+    assert len(fixed) == 1
+    base = fixed.pop()
+    assert 48 < base < 4096
+    r = d.registry_new(10, False)
+    d.registry_del(r, False)
+    assert d.registry_mem(r, False) == base - 48  # the 48-byte scalar block is gone

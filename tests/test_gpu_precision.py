@@ -17,6 +17,9 @@ def test_per_layer_fidelity(dk_gpu):
     assert out["worst"]["min_fidelity"] > 1 - 1e-6
     assert out["worst"]["max_amp_err"] < 5e-5
     assert out["worst"]["max_prob_err"] < 5e-6
+    # the fused whole-circuit runs (no per-layer flush) agree as well
+    assert out["fused_final"]["fidelity"] > 1 - 1e-6
+    assert out["c64_layers_per_s_fused"] > 0 and out["c128_layers_per_s_fused"] > 0
 
 
 def test_compare_matches_host_computation(dk_gpu):

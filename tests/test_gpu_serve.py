@@ -74,3 +74,32 @@ def test_join_across_slots(dk_gpu, orc):
     ob = W.run_ops(orc, orc.registry_new(5), W.small_circuit(seed=41, n=5, depth=3).ops)
     assert np.allclose(d.registry_get_all(j), orc.registry_get_all(orc.registry_join(oa, ob)),
                        atol=ATOL_C128)
+
+
+@pytest.mark.parametrize("after", ["del", "overwrite"])
+def test_join_across_slots_then_reuse_least(dk_gpu, after):
+    """A join reads the least register's storage on the most register's
+    stream.  Work that least's slot queues right after the join -- freeing
+    that storage (and a new register reusing the pool block), or a register
+    derived from least flushed in place over it -- must wait for that read."""
+    d = dk_gpu
+    s1, s2 = d.engine_new_slot(), d.engine_new_slot()
+    d.engine_set_slot(s1)
+    a = W.run_ops(d, d.registry_new(2, False), W.small_circuit(seed=42, n=2, depth=2).ops)
+    d.engine_set_slot(s2)
+    b = W.run_ops(d, d.registry_new(24, False), W.small_circuit(seed=43, n=24, depth=1).ops)
+    d.engine_set_slot(0)
+    va, vb = d.registry_get_all(a, False), d.registry_get_all(b, False)
+    j = d.registry_join(a, b, 1, False)
+    if after == "del":
+        d.registry_del(b, False)
+        d.engine_set_slot(s2)
+        reuse = d.registry_new(24, False)
+        d.engine_set_slot(0)
+        assert d.registry_prob(reuse, 0, 1, False) == 0.0
+    else:
+        g = d.gate_new(1, W.u3(0.3, 0.2, 0.1).tolist(), False)
+        b2 = d.registry_apply(b, g, [0], None, None, 1, False)
+        del b  # b2 alone holds the storage: its sweep runs in place
+        d.registry_prob(b2, 0, 1, False)
+    assert np.allclose(d.registry_get_all(j, False), np.kron(va, vb), atol=ATOL_C128, rtol=0)

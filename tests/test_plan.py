@@ -573,3 +573,20 @@ def test_chained_pairs_fill_for_few_wavefronts(lib, prec, res, bound):
                 pairs += 1
     assert pairs > 100
     assert total <= bound * 2 * pairs, (total, pairs)
+
+
+def test_plan_unfused_keeps_controls_out_of_the_tile(lib):
+    """One gate per sweep: the gate's controls and anticontrols stay outside
+    the tile (tile conditions), so an in-place sweep moves only the tiles
+    where they hold (2 S 2^-c bytes); the pinned low qubits stay in."""
+    c = W.scale_circuit(seed=2, n=30, depth=2)
+    steps, blob = build_plan(lib, c.ops, 30, fuse=0)
+    assert len(steps) == len(c.ops)
+    for (kind, off, _), op in zip(steps, c.ops):
+        assert kind == 1
+        h = np.frombuffer(blob, HDR, 1, off)[0]
+        tile = set(int(q) for q in h["qpos"][:h["m"]])
+        assert {0, 1} <= tile and set(op.targets) <= tile
+        cond = (op.controls | op.anticontrols) - {0, 1}
+        assert not (cond & tile), (op.targets, op.controls, op.anticontrols)
+        assert bool(h["all_touched"]) == (not cond)

@@ -37,6 +37,15 @@ def random_state(rng, n):
     return v / np.linalg.norm(v)
 
 
+def torch_marginals(amps, n):
+    """Plain PyTorch FP64 restatement of the reduction: out[q] = sum of
+    |a_i|^2 over i with bit q set, out[n] = the total."""
+    import torch
+    p = amps.to(torch.complex128).abs().pow(2)
+    out = [p.view(1 << (n - 1 - q), 2, 1 << q)[:, 1, :].sum().item() for q in range(n)]
+    return np.array(out + [p.sum().item()])
+
+
 @pytest.mark.parametrize("precision", [2, 1])
 def test_noalloc_marginals_match_allocating_entry_point(dk_gpu, precision):
     import torch
@@ -46,8 +55,11 @@ def test_noalloc_marginals_match_allocating_entry_point(dk_gpu, precision):
     rng = np.random.default_rng(2024 + precision)
     host_dtype = np.complex128 if precision == 2 else np.complex64
     stream = torch.cuda.current_stream().cuda_stream
-    # two calls in a row, different sizes: leftover scratch must not leak in
-    for n in (20, 17):
+    tol = ATOL_C128 if precision == 2 else 1e-6
+    # calls in a row, different sizes: leftover scratch must not leak in.
+    # n = 3 and 6 run one warp with idle lanes; 17 and 20 the block-limited
+    # grid with 12 accumulated bits per thread.
+    for n in (20, 3, 17, 6):
         v = random_state(rng, n)
         host = np.ascontiguousarray(v.astype(host_dtype))
         amps = torch.from_numpy(host.view(np.float64 if precision == 2 else np.float32)).cuda()
@@ -59,10 +71,36 @@ def test_noalloc_marginals_match_allocating_entry_point(dk_gpu, precision):
         # the allocating entry point on a register holding the same values
         reg = d.registry_new_data(n, host.astype(np.complex128), False, precision)
         want = np.array(d.registry_probs(reg))  # norm = 1: raw sums, as the reference
-        tol = ATOL_C128 if precision == 2 else 1e-6
         assert np.allclose(got[:n], want, atol=tol, rtol=0)
+        # and numpy on the stored values, qubit by qubit
         stored = np.abs(host.astype(np.complex128)) ** 2
+        idx = np.arange(1 << n)
+        for q in range(n):
+            assert abs(got[q] - stored[(idx >> q) & 1 == 1].sum()) < tol, (n, q)
         assert abs(got[n] - stored.sum()) < tol
+
+
+def test_noalloc_marginals_wide_accumulators(dk_gpu):
+    """29 qubits complex64 (4 GiB): 256 blocks of 256 threads leave 13 bits
+    per thread, the kernel variant with 16 accumulators.  Checked against a
+    plain PyTorch FP64 reduction of the same device array, twice in a row."""
+    import torch
+
+    lib = noalloc_lib()
+    n = 29
+    gen = torch.Generator(device="cuda").manual_seed(29)
+    amps = torch.randn(1 << n, dtype=torch.complex64, device="cuda", generator=gen)
+    amps /= amps.abs().pow(2).sum().sqrt()
+    want = torch_marginals(amps, n)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        out = torch.full((n + 1,), float("nan"), dtype=torch.float64, device="cuda")
+        rc = lib.dk_marginals_noalloc(amps.data_ptr(), n, 1, out.data_ptr(), stream)
+        assert rc == 0
+        torch.cuda.synchronize()
+        assert np.allclose(out.cpu().numpy(), want, atol=1e-9, rtol=0)
+    del amps
+    torch.cuda.empty_cache()
 
 
 def test_noalloc_rejects_oversized_registers():

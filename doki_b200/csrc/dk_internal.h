@@ -234,6 +234,10 @@ int dk_gate_classify(const struct dk_gate *g);
  * kernel index check since the last reset, 0 if none (site in bits 56-63,
  * index in bits 0-55). */
 int dk_debug_checks(uint64_t *first_failure, int reset);
+/* Debug builds only: 1 starves every later tcgen05 sweep of its MMA
+ * completions (its bounded waits expire: DK_ERR_TIMEOUT at the next read),
+ * 0 restores normal operation. */
+int dk_debug_tm_starve(int on);
 
 #ifdef __cplusplus
 }

@@ -758,6 +758,423 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 	}
 }
 
+/* ---- complex64 tensor sweep on tcgen05 (tensor memory) --------------------
+ *
+ * The same sweep programs as k_sweep_tc (12-bit tiles, every entry an 8x8
+ * complex matrix in register order), with each entry applied by the 5th-gen
+ * tensor cores.  The 512 columns of a tile (8 amplitudes that differ only in
+ * the pass bits) are the rows of A; one entry is
+ *     Y^T (512 x 16) = X^T (512 x 16) R^T,   R = [[Mr, -Mi], [Mi, Mr]],
+ * x = (re0..re7, im0..im7) of a column, as 4 row blocks of M = 128 (one
+ * tensor-memory lane per column), N = 16, K = 16 (two k-steps of 8).
+ * Operands are split into TF32 hi + lo parts (as in the mma.sync form) and
+ * each block takes lo*hi + hi*lo + hi*hi, accumulated in FP32 in tensor
+ * memory.  A lives in tensor memory (written by the threads that gathered
+ * the columns, tcgen05.st), B (R^T hi / lo, 1 KiB each) in shared memory in
+ * the K-major layout without swizzle, D in tensor memory; one thread issues
+ * the 24 MMAs and commits them to an mbarrier, and every thread reads back
+ * its own rows (tcgen05.ld), so a column never leaves the thread that owns
+ * it between gather and scatter.
+ *
+ * Tensor-memory columns per CTA (256): A hi [0, 64), A lo [64, 128),
+ * D [128, 192) -- 16 per row block.  The launch keeps at most two CTAs of
+ * any such kernel per SM (shared memory), so 2 x 256 <= 512 columns and the
+ * allocation never waits.  Warp w owns row blocks 2 (w / 4) and
+ * 2 (w / 4) + 1 in lanes 32 (w % 4) .. + 31: column c = 128 b + 32 (w % 4) +
+ * lane.  Every wait on the MMAs is bounded: on expiry the kernel counts the
+ * fault in g_dk_tm_fault, waits (bounded) for the MMAs in flight, frees its
+ * tensor memory and returns; the host reports DK_ERR_TIMEOUT at the next
+ * read. */
+__device__ unsigned int g_dk_tm_fault;
+#ifdef DK_DEBUG_CHECKS
+/* Debug builds only, a test hook: while set, the issuing thread of a tcgen05
+ * sweep issues no MMA and no commit, so every wait runs out on an mbarrier
+ * that nothing arrives at (dk_debug_tm_starve). */
+__device__ int g_dk_tm_starve;
+#define DK_TM_STARVED() (g_dk_tm_starve != 0)
+#else
+#define DK_TM_STARVED() false
+#endif
+
+constexpr int kTmCols = 256; /* tensor-memory columns per CTA */
+/* A wait on the MMAs gives up after this long (ns of %globaltimer); the
+ * poll count is a second bound in case the timer does not advance. */
+constexpr unsigned long long kTmWaitNs = 1000000000ull;
+constexpr int kTmWaitPolls = 1 << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+	return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+/* Shared-memory matrix descriptor: K-major, no swizzle, core matrices of 8
+ * rows x 16 bytes; LBO = 128 B between the two 16-byte K chunks of a k-step,
+ * SBO = 256 B between 8-row groups; descriptor version 1. */
+__device__ __forceinline__ uint64_t umma_desc_k(uint32_t addr)
+{
+	return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(128u >> 4) << 16) |
+	       ((uint64_t)(256u >> 4) << 32) | ((uint64_t)1 << 46);
+}
+
+/* Offset (in floats) of R(n, k) in a B buffer of that layout: k-steps of 8
+ * at 128 floats (512 B), 8-row groups at 64, K chunks of 4 at 32, rows at 4. */
+__device__ __forceinline__ int umma_b_off(int n, int k)
+{
+	return (k >> 3) * 128 + (n >> 3) * 64 + ((k & 7) >> 2) * 32 + (n & 7) * 4 + (k & 3);
+}
+
+/* kind::tf32, D f32, A and B K-major, M = 128, N = 16 */
+constexpr uint32_t kTmIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((16u >> 3) << 17) |
+			      ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma_tf32_ts(uint32_t d, uint32_t a, uint64_t b, uint32_t acc)
+{
+	const uint32_t zero = 0;
+	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+		     "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+		     ::"r"(d), "r"(a), "l"(b), "r"(kTmIdesc), "r"(acc), "r"(zero));
+}
+
+__device__ __forceinline__ void tm_st16(uint32_t ta, const uint32_t (&v)[16])
+{
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, "
+		     "%8, %9, %10, %11, %12, %13, %14, %15, %16};" ::"r"(ta),
+		     "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),
+		     "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]),
+		     "r"(v[14]), "r"(v[15]));
+}
+
+__device__ __forceinline__ void tm_ld16(uint32_t ta, uint32_t (&v)[16])
+{
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, "
+		     "%9, %10, %11, %12, %13, %14, %15}, [%16];"
+		     : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+		       "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+		       "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+		     : "r"(ta));
+}
+
+/* Wait for the mbarrier's phase `parity` to complete, for at most kTmWaitNs
+ * (and kTmWaitPolls polls); false when the limit ran out. */
+__device__ __forceinline__ bool tm_wait(uint32_t mbar, uint32_t parity)
+{
+	unsigned long long t0, t1;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+	for (int it = 0; it < kTmWaitPolls; ++it) {
+		uint32_t done;
+		asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+			     "selp.u32 %0, 1, 0, p;\n\t}"
+			     : "=r"(done)
+			     : "r"(mbar), "r"(parity));
+		if (done)
+			return true;
+		asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+		if (t1 - t0 > kTmWaitNs)
+			return false;
+	}
+	return false;
+}
+
+template <int SW>
+__global__ void __launch_bounds__(256, 2)
+	k_sweep_tm(const float2 *__restrict__ in, float2 *out, const unsigned char *__restrict__ prog,
+		   double *partials)
+{
+	typedef float2 C2;
+	constexpr int M = 12;
+	extern __shared__ __align__(16) unsigned char sm[];
+	const dk_sweep_hdr *h = reinterpret_cast<const dk_sweep_hdr *>(prog);
+	const int m = h->m; /* == 12 (checked by the launcher) */
+	const int lanes = m - PB;
+	const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+	const int npass = h->npass, ngate = h->ngate;
+	const uint32_t tn_amp = 1u << M;
+	const int ncond = (int)h->ncond;
+	const size_t gate_bytes = (size_t)ngate * sizeof(dk_gate_desc);
+	C2 *const tile = reinterpret_cast<C2 *>(sm);
+	uint4 *sg = reinterpret_cast<uint4 *>(sm + sizeof(C2) * tn_amp);
+	dk_gate_cond *scond =
+		reinterpret_cast<dk_gate_cond *>(reinterpret_cast<unsigned char *>(sg) + gate_bytes);
+	const dk_pass_desc *passes = reinterpret_cast<const dk_pass_desc *>(prog + h->pass_off);
+	const double2 *mats = reinterpret_cast<const double2 *>(prog + h->mat_off);
+	__shared__ __align__(1024) float sB[2][256]; /* R^T hi, lo */
+	__shared__ __align__(8) uint64_t mbar;
+	__shared__ uint32_t tslot;
+	__shared__ uint8_t sq[16];
+	__shared__ uint64_t soff[NA];
+	__shared__ uint32_t sro[NA];
+	__shared__ uint64_t sdep[DK_DEP_NIBBLES][16];
+
+	{
+		const uint4 *src = reinterpret_cast<const uint4 *>(prog + h->gate_off);
+		for (int i = tid; i < ngate; i += blockDim.x)
+			sg[i] = __ldg(src + i);
+		const uint4 *csrc = reinterpret_cast<const uint4 *>(prog + h->cond_off);
+		uint4 *cdst = reinterpret_cast<uint4 *>(scond);
+		for (int i = tid; i < ncond; i += blockDim.x)
+			cdst[i] = __ldg(csrc + i);
+		for (int i = tid; i < 16; i += blockDim.x)
+			sq[i] = h->qpos[i];
+	}
+	if (tid == 0) {
+		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+		asm volatile("fence.mbarrier_init.release.cluster;" ::);
+	}
+	if (warp == 0) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+				     smem_u32(&tslot)),
+			     "r"(kTmCols));
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+	}
+	asm volatile("tcgen05.fence::before_thread_sync;" ::);
+	__syncthreads();
+	asm volatile("tcgen05.fence::after_thread_sync;" ::);
+	const uint32_t tbase = tslot;
+	for (int r = tid; r < NA; r += blockDim.x) {
+		uint64_t o = 0;
+		for (int j = 0; j < PB; ++j)
+			if ((r >> j) & 1)
+				o |= 1ull << sq[lanes + j];
+		soff[r] = o;
+		sro[r] = swz<SW>((uint32_t)r << lanes);
+	}
+	for (int e = tid; e < DK_DEP_NIBBLES * 16; e += blockDim.x) {
+		uint64_t v = (uint64_t)(e & 15) << (4 * (e >> 4));
+		for (int j = 0; j < m; ++j) {
+			const int q = sq[j];
+			v = ((v >> q) << (q + 1)) | (v & ((1ull << q) - 1ull));
+		}
+		sdep[e >> 4][e & 15] = v;
+	}
+	/* streaming: thread t owns tile columns t and t + 256 (as k_sweep_tc) */
+	uint64_t off_t0 = 0;
+	for (int j = 0; j < lanes; ++j)
+		if ((tid >> j) & 1u)
+			off_t0 |= 1ull << sq[j];
+	const uint32_t stid0 = swz<SW>(tid);
+	auto off_t = [&](int hh) -> uint64_t { return hh ? (off_t0 | (1ull << sq[8])) : off_t0; };
+	auto stid = [&](int hh) -> uint32_t { return hh ? (stid0 ^ swz<SW>(256u)) : stid0; };
+	/* passes: this thread's columns, one per row block it owns */
+	const uint32_t rb0 = 2u * (warp >> 2);
+	uint32_t col[2];
+	col[0] = 128u * rb0 + 32u * (warp & 3u) + lane;
+	col[1] = col[0] + 128u;
+	const uint32_t ta = tbase + ((32u * (warp & 3u)) << 16); /* this warp's lane quarter */
+	const uint32_t mb = smem_u32(&mbar);
+	const uint32_t sb_hi = smem_u32(&sB[0][0]), sb_lo = smem_u32(&sB[1][0]);
+	__syncthreads();
+	const uint64_t ntiles = h->ntiles;
+	const int ndep = (h->n - m + 3) >> 2;
+	const bool skip_idle = (in == out) && !h->all_touched;
+
+	auto tile_base = [&](uint64_t t) -> uint64_t {
+		uint64_t base = 0;
+#pragma unroll
+		for (int k = 0; k < DK_DEP_NIBBLES; ++k)
+			if (k < ndep)
+				base |= sdep[k][(t >> (4 * k)) & 15u];
+		return base;
+	};
+	auto next_tile = [&](uint64_t t) -> uint64_t {
+		for (; t < ntiles; t += gridDim.x) {
+			if (!skip_idle)
+				return t;
+			const uint64_t base = tile_base(t);
+			for (int g = 0; g < ngate; ++g) {
+				const uint32_t gi = sg[g].y & 0xffffu;
+				if (gi == 0xffffu)
+					return t;
+				const dk_gate_cond c = scond[gi];
+				if (((base & c.gc) == c.gc) && !(base & c.ga))
+					return t;
+			}
+		}
+		return ntiles;
+	};
+	[[maybe_unused]] const uint64_t nglob = 1ull << h->n;
+	auto prefetch = [&](uint64_t base) {
+#pragma unroll
+		for (int hh = 0; hh < 2; ++hh) {
+			const uint64_t bo = base | off_t(hh);
+#pragma unroll
+			for (int r = 0; r < NA; ++r) {
+				const uint32_t so = stid(hh) ^ sro[r];
+				const uint64_t gi = bo | soff[r];
+				if (!DK_IN_BOUNDS(so, tn_amp, CHK_LOAD_SMEM) ||
+				    !DK_IN_BOUNDS(gi, nglob, CHK_LOAD_GLOBAL))
+					continue;
+				cp_async8(tile + so, in + gi);
+			}
+		}
+		cp_async_commit();
+	};
+
+	double insq = 0.0, outsq = 0.0;
+	uint32_t phase = 0;
+	bool fault = false;
+	uint64_t t = next_tile(blockIdx.x);
+	if (t < ntiles)
+		prefetch(tile_base(t));
+	while (t < ntiles && !fault) {
+		const uint64_t base = tile_base(t);
+		uint64_t tn = ntiles;
+		cp_async_wait_all();
+		__syncthreads();
+		if (skip_idle) {
+#pragma unroll
+			for (int hh = 0; hh < 2; ++hh)
+#pragma unroll
+				for (int r = 0; r < NA; ++r) {
+					const uint32_t so = stid(hh) ^ sro[r];
+					if (DK_IN_BOUNDS(so, tn_amp, CHK_READOUT))
+						insq += sqabs(tile[so]);
+				}
+			__syncthreads();
+		}
+		for (int p = 0; p < npass && !fault; ++p) {
+			const dk_pass_desc *pd = passes + p;
+			const uint32_t s0 = __ldg(&pd->sp[0]), s1 = __ldg(&pd->sp[1]),
+				       s2 = __ldg(&pd->sp[2]);
+			uint32_t cs[2];
+#pragma unroll
+			for (int j = 0; j < 2; ++j)
+				cs[j] = __ldg(&pd->slo[col[j] & 31u]) ^ __ldg(&pd->shi[col[j] >> 5]);
+			const int g1 = __ldg(&pd->g1);
+			for (int g = __ldg(&pd->g0); g < g1; ++g) {
+				const uint4 d = sg[g];
+				const uint32_t gi = d.y & 0xffffu;
+				if (gi != 0xffffu) {
+					const dk_gate_cond c = scond[gi];
+					if (((base & c.gc) != c.gc) || (base & c.ga))
+						continue; /* the same for every thread */
+				}
+				const double2 *mt = mats + 64 * (size_t)tc_matrix(d, scond, base);
+				{ /* B = R, entry (n, k), split into hi and lo */
+					const int n = (int)(tid >> 4), k = (int)(tid & 15u);
+					const double2 e = __ldg(mt + 8 * (n & 7) + (k & 7));
+					const float v = ((n < 8) == (k < 8)) ? (float)e.x
+						       : (n < 8 ? -(float)e.y : (float)e.y);
+					uint32_t hi, lo;
+					tf32_split(v, hi, lo);
+					const int o = umma_b_off(n, k);
+					sB[0][o] = __uint_as_float(hi);
+					sB[1][o] = __uint_as_float(lo);
+				}
+#pragma unroll
+				for (int j = 0; j < 2; ++j) {
+					uint32_t vh[16], vl[16];
+#pragma unroll
+					for (int r = 0; r < NA; ++r) {
+						const uint32_t so = cs[j] ^ ((r & 1) ? s0 : 0u) ^
+								    ((r & 2) ? s1 : 0u) ^ ((r & 4) ? s2 : 0u);
+						const C2 x = DK_IN_BOUNDS(so, tn_amp, CHK_GATHER) ? tile[so] : C2{};
+						tf32_split(x.x, vh[r], vl[r]);
+						tf32_split(x.y, vh[8 + r], vl[8 + r]);
+					}
+					const uint32_t rb = rb0 + (uint32_t)j;
+					tm_st16(ta + 16u * rb, vh);
+					tm_st16(ta + 64u + 16u * rb, vl);
+				}
+				asm volatile("tcgen05.wait::st.sync.aligned;" ::);
+				asm volatile("fence.proxy.async.shared::cta;" ::);
+				asm volatile("tcgen05.fence::before_thread_sync;" ::);
+				__syncthreads();
+				if (tid == 0 && !DK_TM_STARVED()) {
+					asm volatile("tcgen05.fence::after_thread_sync;" ::);
+					const uint64_t bh0 = umma_desc_k(sb_hi), bh1 = umma_desc_k(sb_hi + 512u);
+					const uint64_t bl0 = umma_desc_k(sb_lo), bl1 = umma_desc_k(sb_lo + 512u);
+#pragma unroll
+					for (uint32_t rb = 0; rb < 4; ++rb) {
+						const uint32_t dcol = tbase + 128u + 16u * rb;
+						const uint32_t ah = tbase + 16u * rb, al = tbase + 64u + 16u * rb;
+						/* small terms first */
+						umma_tf32_ts(dcol, al, bh0, 0u);
+						umma_tf32_ts(dcol, al + 8u, bh1, 1u);
+						umma_tf32_ts(dcol, ah, bl0, 1u);
+						umma_tf32_ts(dcol, ah + 8u, bl1, 1u);
+						umma_tf32_ts(dcol, ah, bh0, 1u);
+						umma_tf32_ts(dcol, ah + 8u, bh1, 1u);
+					}
+					asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+						     ::"r"(mb));
+				}
+				const bool ok = tm_wait(mb, phase);
+				phase ^= 1u;
+				asm volatile("tcgen05.fence::after_thread_sync;" ::);
+				const bool ctl = (d.x & 0xffffu) == DK_GC_DENSE3 + 1;
+#pragma unroll
+				for (int j = 0; j < 2; ++j) {
+					uint32_t y[16];
+					tm_ld16(ta + 128u + 16u * (rb0 + (uint32_t)j), y);
+					asm volatile("tcgen05.wait::ld.sync.aligned;" ::);
+					if (!ok)
+						continue;
+					if (ctl) { /* rare: controls off the pass bits */
+						const uint32_t raw = __ldg(&pd->rlo[col[j] & 31u]) |
+								     __ldg(&pd->rhi[col[j] >> 5]);
+						if (!ctl_ok(raw, d.z, d.w))
+							continue;
+					}
+#pragma unroll
+					for (int r = 0; r < NA; ++r) {
+						const uint32_t so = cs[j] ^ ((r & 1) ? s0 : 0u) ^
+								    ((r & 2) ? s1 : 0u) ^ ((r & 4) ? s2 : 0u);
+						if (DK_IN_BOUNDS(so, tn_amp, CHK_SCATTER))
+							tile[so] = make_float2(__uint_as_float(y[r]),
+									       __uint_as_float(y[8 + r]));
+					}
+				}
+				/* the scatters precede the next gather and the B rewrite;
+				 * a timeout anywhere stops every thread */
+				asm volatile("tcgen05.fence::before_thread_sync;" ::);
+				if (__syncthreads_or(!ok)) {
+					fault = true;
+					break;
+				}
+			}
+		}
+		if (fault)
+			break;
+#pragma unroll
+		for (int hh = 0; hh < 2; ++hh) {
+			const uint64_t bo = base | off_t(hh);
+#pragma unroll
+			for (int r = 0; r < NA; ++r) {
+				const uint32_t so = stid(hh) ^ sro[r];
+				const C2 v = DK_IN_BOUNDS(so, tn_amp, CHK_READOUT) ? tile[so] : C2{};
+				outsq += sqabs(v);
+				if (DK_IN_BOUNDS(bo | soff[r], nglob, CHK_STORE))
+					__stcs(out + (bo | soff[r]), v);
+			}
+		}
+		__syncthreads(); /* the buffer is free */
+		tn = next_tile(t + gridDim.x);
+		if (tn < ntiles)
+			prefetch(tile_base(tn));
+		t = tn;
+	}
+	cp_async_wait_all();
+	if (fault) {
+		/* the MMAs of the expired wait may still run: give them another
+		 * bounded wait before the tensor memory is released */
+		if (tid == 0) {
+			atomicAdd(&g_dk_tm_fault, 1u);
+			(void)tm_wait(mb, phase ^ 1u);
+		}
+		insq = outsq = __longlong_as_double(0x7ff8000000000000ll);
+	}
+	asm volatile("tcgen05.fence::before_thread_sync;" ::);
+	__syncthreads();
+	if (warp == 0)
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase),
+			     "r"(kTmCols));
+	block_sum2(insq, outsq);
+	if (tid == 0) {
+		partials[2 * blockIdx.x] = insq;
+		partials[2 * blockIdx.x + 1] = outsq;
+	}
+}
+
 enum { FIN_GATE = 0, FIN_COLLAPSE = 1, FIN_RESET = 2 };
 
 /* Sum the (in, out) partials of `nb` blocks in a fixed order and update the
@@ -1668,6 +2085,8 @@ int g_num_sms = 148;
 } // namespace
 
 std::atomic<unsigned long long> g_launches{0};
+int g_c64_tmem = 1;
+std::atomic<int> g_tm_ran{0};
 
 /* ---------------------------------------------------------------------- */
 
@@ -1753,6 +2172,71 @@ static cudaError_t run_sweep_tc(const void *in, void *out, const unsigned char *
 	return cudaGetLastError();
 }
 
+/* Dynamic shared memory of a k_sweep_tm CTA: at least this much, so that no
+ * SM holds more than two CTAs of it (or of any kernel with the same floor)
+ * and their 2 x 256 tensor-memory columns always fit in the SM's 512. */
+constexpr size_t kTmSmemFloor = 80u << 10;
+
+static cudaError_t run_sweep_tm(const void *in, void *out, const unsigned char *dprog,
+				const dk_sweep_hdr *hp, int num_sms, const Scratch &s,
+				cudaStream_t st, int *blocks_out)
+{
+	size_t smem = (sizeof(float2) << 12) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
+		      (size_t)hp->ncond * sizeof(dk_gate_cond);
+	if (smem < kTmSmemFloor)
+		smem = kTmSmemFloor;
+	auto kern = k_sweep_tm<4>;
+	/* raised once to the device maximum, never lowered (see run_sweep) */
+	static std::once_flag once;
+	static cudaError_t set_err = cudaSuccess;
+	std::call_once(once, [&] {
+		int dev = 0, maxopt = 0;
+		cudaGetDevice(&dev);
+		set_err = cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+						 dev);
+		cudaFuncAttributes fa;
+		if (set_err == cudaSuccess)
+			set_err = cudaFuncGetAttributes(&fa, kern);
+		if (set_err == cudaSuccess)
+			set_err = cudaFuncSetAttribute(kern,
+						       cudaFuncAttributeMaxDynamicSharedMemorySize,
+						       maxopt - (int)fa.sharedSizeBytes);
+	});
+	cudaError_t e = set_err;
+	if (e != cudaSuccess)
+		return e;
+	uint64_t blocks = hp->ntiles;
+	const uint64_t cap = (uint64_t)num_sms * 2;
+	if (blocks > cap)
+		blocks = cap;
+	kern<<<(int)blocks, 256, smem, st>>>((const float2 *)in, (float2 *)out, dprog,
+					     s.partials);
+	*blocks_out = (int)blocks;
+	g_tm_ran.store(1);
+	return cudaGetLastError();
+}
+
+cudaError_t tm_fault_check(cudaStream_t st, unsigned *faults)
+{
+	*faults = 0;
+	if (!g_tm_ran.load())
+		return cudaSuccess;
+	unsigned v = 0;
+	cudaError_t e = cudaMemcpyFromSymbolAsync(&v, g_dk_tm_fault, sizeof(v), 0,
+						  cudaMemcpyDeviceToHost, st);
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(st);
+	if (e == cudaSuccess && v) {
+		const unsigned zero = 0;
+		e = cudaMemcpyToSymbolAsync(g_dk_tm_fault, &zero, sizeof(zero), 0,
+					    cudaMemcpyHostToDevice, st);
+		if (e == cudaSuccess)
+			e = cudaStreamSynchronize(st);
+	}
+	*faults = v;
+	return e;
+}
+
 cudaError_t launch_sweep(int prec, const void *in, void *out,
 			 const unsigned char *dprog, const dk_sweep_hdr *hp,
 			 const dk_scal *sc_in, dk_scal *sc_out, const Scratch &s,
@@ -1762,6 +2246,16 @@ cudaError_t launch_sweep(int prec, const void *in, void *out,
 	const int m = hp->m;
 	int blocks = 0;
 	cudaError_t e;
+	if (hp->mode == DK_SWEEP_TENSOR && prec == DK_C64 && m == 12 && g_c64_tmem) {
+		/* complex64, 12-bit tiles: tcgen05 TF32 products in tensor memory */
+		e = run_sweep_tm(in, out, dprog, hp, num_sms, s, st, &blocks);
+		if (e != cudaSuccess)
+			return e;
+		const int all = hp->all_touched || (in != out);
+		k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc_in, sc_out, FIN_GATE, all);
+		g_launches += 2;
+		return cudaGetLastError();
+	}
 	if (hp->mode == DK_SWEEP_TENSOR) {
 		/* tensor-core passes (FP64 for complex128, split TF32 for
 		 * complex64); tiles of 8 to 12 bits */
@@ -2346,6 +2840,19 @@ extern "C" int dk_debug_checks(uint64_t *first_failure, int reset)
 	}
 	if (first_failure)
 		*first_failure = v;
+	return DK_OK;
+}
+
+/* Debug builds only: 1 makes every later tcgen05 sweep wait on an mbarrier
+ * that nothing arrives at (its bounded waits expire and the next read of
+ * the register returns DK_ERR_TIMEOUT); 0 restores normal operation. */
+extern "C" int dk_debug_tm_starve(int on)
+{
+	const int v = on ? 1 : 0;
+	if (cudaMemcpyToSymbol(dk::g_dk_tm_starve, &v, sizeof(v)) != cudaSuccess) {
+		cudaGetLastError();
+		return DK_ERR_CUDA;
+	}
 	return DK_OK;
 }
 #endif

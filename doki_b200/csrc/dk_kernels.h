@@ -15,6 +15,15 @@ namespace dk {
  * Several slot threads launch at once, so the count is atomic: it orders
  * nothing, it only must not lose increments. */
 extern std::atomic<unsigned long long> g_launches;
+/* complex64 tensor sweeps of 12-bit tiles on tcgen05 (1, default) or on the
+ * mma.sync split-TF32 kernel (0) */
+extern int g_c64_tmem;
+/* set once a tcgen05 sweep has been launched (tm_fault_check has work) */
+extern std::atomic<int> g_tm_ran;
+
+/* Faults counted by tcgen05 sweeps whose bounded waits expired since the
+ * last call (0 = none); reads and clears the device counter on `st`. */
+cudaError_t tm_fault_check(cudaStream_t st, unsigned *faults);
 
 /* Number of per-block partial slots the scratch buffer must hold. */
 constexpr int kMaxBlocks = 4096;

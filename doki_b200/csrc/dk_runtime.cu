@@ -399,6 +399,15 @@ int read_scal(dk_state *s)
 	CK(cudaMemcpyAsync(&sc, s->buf->sc, sizeof(sc), cudaMemcpyDeviceToHost, CUR.st));
 	g.d2h += sizeof(sc);
 	CK(cudaStreamSynchronize(CUR.st));
+	/* a tcgen05 sweep whose bounded wait expired left the register's
+	 * content undefined: report it instead of reading it */
+	unsigned faults = 0;
+	CK(dk::tm_fault_check(CUR.st, &faults));
+	if (faults) {
+		snprintf(g.err, sizeof(g.err), "tensor-memory sweep: %u bounded waits expired",
+			 faults);
+		return DK_ERR_TIMEOUT;
+	}
 	s->norm = sc.norm;
 	s->csq = sc.csq;
 	s->have_norm = 1;
@@ -538,6 +547,9 @@ int dk_init(int device)
 	const char *te = getenv("DK_TENSOR");
 	if (te)
 		g.tensor = atoi(te) ? 0 : -1;
+	const char *tm = getenv("DK_C64_TMEM");
+	if (tm)
+		dk::g_c64_tmem = atoi(tm) ? 1 : 0;
 	g.inited = 1;
 	return DK_OK;
 }
@@ -817,6 +829,74 @@ int dk_apply_gate(dk_state *in, const dk_gate *gate, const unsigned *targets,
 	s->buf->refcount++;
 	s->pending = op;
 	*out = s;
+	return DK_OK;
+}
+
+int dk_apply_gates(dk_state *in, unsigned count, const unsigned *op_k,
+		   const unsigned *op_targets, const uint64_t *op_controls,
+		   const uint64_t *op_anticontrols, const uint64_t *op_matrix,
+		   const double *matrices, uint64_t num_matrix_entries, dk_state **out)
+{
+	DK_TRACE();
+	if (!in || !out || (count && (!op_k || !op_targets || !op_controls || !op_anticontrols ||
+				      !op_matrix || !matrices)))
+		return DK_ERR_ARG;
+	int rc = check_live(in);
+	if (rc)
+		return rc;
+	if (in->n == 0 || !in->buf)
+		return DK_ERR_EMPTY;
+	const uint64_t full = (in->n >= 64) ? ~0ull : ((1ull << in->n) - 1ull);
+	/* validate everything first: a failed call queues nothing */
+	for (unsigned i = 0; i < count; ++i) {
+		const unsigned k = op_k[i];
+		if (k == 0 || k > 3)
+			return DK_ERR_ARG;
+		uint64_t used = 0;
+		for (unsigned j = 0; j < k; ++j) {
+			const unsigned t = op_targets[3 * i + j];
+			if (t >= in->n || ((used >> t) & 1u))
+				return DK_ERR_ARG;
+			used |= 1ull << t;
+		}
+		const uint64_t cm = op_controls[i], am = op_anticontrols[i];
+		if ((cm | am) & ~full || (cm & am) || ((cm | am) & used))
+			return DK_ERR_ARG;
+		if (op_matrix[i] > num_matrix_entries ||
+		    (1ull << (2 * k)) > num_matrix_entries - op_matrix[i])
+			return DK_ERR_ARG;
+	}
+	dk_state *cur = in;
+	for (unsigned i = 0; i < count; ++i) {
+		const unsigned k = op_k[i];
+		dk_gate *g = nullptr;
+		rc = dk_gate_new(k, matrices + 2 * op_matrix[i], &g);
+		if (rc)
+			break;
+		unsigned ctl[64], act[64], nc = 0, na = 0;
+		for (unsigned q = 0; q < in->n; ++q) {
+			if ((op_controls[i] >> q) & 1u)
+				ctl[nc++] = q;
+			if ((op_anticontrols[i] >> q) & 1u)
+				act[na++] = q;
+		}
+		dk_state *next = nullptr;
+		rc = dk_apply_gate(cur, g, op_targets + 3 * i, k, ctl, nc, act, na, &next);
+		dk_gate_free(g); /* the queued op keeps its own reference */
+		if (rc)
+			break;
+		if (cur != in)
+			dk_state_free(cur);
+		cur = next;
+	}
+	if (rc) {
+		if (cur != in)
+			dk_state_free(cur);
+		return rc;
+	}
+	if (cur == in)
+		return dk_state_clone(in, out);
+	*out = cur;
 	return DK_OK;
 }
 

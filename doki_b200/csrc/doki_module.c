@@ -1049,6 +1049,88 @@ done:
 	return res;
 }
 
+/* A C-contiguous buffer of `count` items of `itemsize` bytes (count < 0:
+ * any length; the length is returned through *len). */
+static int get_array(PyObject *obj, Py_buffer *view, Py_ssize_t itemsize, Py_ssize_t count,
+		     Py_ssize_t *len, const char *name)
+{
+	if (PyObject_GetBuffer(obj, view, PyBUF_C_CONTIGUOUS | PyBUF_FORMAT) != 0) {
+		PyErr_Clear();
+		PyErr_Format(DokiError, "%s must be a contiguous numpy array", name);
+		return -1;
+	}
+	if (view->itemsize != itemsize || (count >= 0 && view->len != count * itemsize)) {
+		PyBuffer_Release(view);
+		PyErr_Format(DokiError, "%s has the wrong item size or length", name);
+		return -1;
+	}
+	if (len)
+		*len = view->len / itemsize;
+	return 0;
+}
+
+/* registry_apply_many(registry, op_k, op_targets, op_controls, op_anticontrols,
+ * op_matrix, matrices): every gate of a circuit in one call (the serving
+ * form's submission path; the reference applies one gate per
+ * registry_apply call, doki.c:722-941).  Arrays as dk_apply_gates takes
+ * them: uint32 op_k [N], uint32 op_targets [N, 3], uint64 op_controls [N],
+ * uint64 op_anticontrols [N], uint64 op_matrix [N], complex128 matrices. */
+static PyObject *doki_registry_apply_many(PyObject *self, PyObject *args)
+{
+	PyObject *scap, *ok, *ot, *oc, *oa, *om, *mats;
+	if (!PyArg_ParseTuple(args, "OOOOOOO", &scap, &ok, &ot, &oc, &oa, &om, &mats)) {
+		PyErr_SetString(DokiError, "Syntax: registry_apply_many(registry, op_k, op_targets, "
+					   "op_controls, op_anticontrols, op_matrix, matrices)");
+		return NULL;
+	}
+	dk_state *s = get_state(scap, "NULL pointer to registry");
+	if (!s)
+		return NULL;
+	Py_buffer vk, vt, vc, va, vm, vx;
+	Py_ssize_t n = 0, nm = 0;
+	if (get_array(ok, &vk, 4, -1, &n, "op_k"))
+		return NULL;
+	PyObject *res = NULL;
+	int got = 1;
+	if (get_array(ot, &vt, 4, 3 * n, NULL, "op_targets"))
+		goto r1;
+	got++;
+	if (get_array(oc, &vc, 8, n, NULL, "op_controls"))
+		goto r2;
+	got++;
+	if (get_array(oa, &va, 8, n, NULL, "op_anticontrols"))
+		goto r3;
+	got++;
+	if (get_array(om, &vm, 8, n, NULL, "op_matrix"))
+		goto r4;
+	got++;
+	if (get_array(mats, &vx, 16, -1, &nm, "matrices"))
+		goto r5;
+	{
+		dk_state *out = NULL;
+		int rc;
+		Py_BEGIN_ALLOW_THREADS rc = dk_apply_gates(
+			s, (unsigned)n, (const unsigned *)vk.buf, (const unsigned *)vt.buf,
+			(const uint64_t *)vc.buf, (const uint64_t *)va.buf, (const uint64_t *)vm.buf,
+			(const double *)vx.buf, (uint64_t)nm, &out);
+		Py_END_ALLOW_THREADS if (rc) raise_dk(rc, "Failed to apply the gates");
+		else res = wrap_state(out);
+	}
+	PyBuffer_Release(&vx);
+r5:
+	PyBuffer_Release(&vm);
+r4:
+	PyBuffer_Release(&va);
+r3:
+	PyBuffer_Release(&vc);
+r2:
+	PyBuffer_Release(&vt);
+r1:
+	PyBuffer_Release(&vk);
+	(void)got;
+	return res;
+}
+
 static PyObject *doki_registry_join(PyObject *self, PyObject *args)
 {
 	PyObject *c1, *c2;
@@ -2214,6 +2296,8 @@ static PyMethodDef DokiMethods[] = {
 	  "Functional column vector after applying a gate to a functional state" },
 	{ "funmatrix_mem", doki_funmatrix_mem, METH_VARARGS,
 	  "Get the memory allocated by this FMatrix in bytes" },
+	{ "registry_apply_many", doki_registry_apply_many, METH_VARARGS,
+	  "Queue every gate of a circuit given as flat arrays (serving form)" },
 	{ "registry_get_all", doki_registry_get_all, METH_VARARGS,
 	  "All amplitudes of a registry as a numpy array" },
 	{ "registry_probs", doki_registry_probs, METH_VARARGS,

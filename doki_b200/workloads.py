@@ -277,3 +277,62 @@ def batch_arrays(seed: int = 4, count: int = 4096, qmin: int = 4, qmax: int = 16
                      np.array(starts, dtype=np.uint64), np.concatenate(ks),
                      np.concatenate(tgs), np.concatenate(cms), np.zeros(n_ops, dtype=np.uint64),
                      np.concatenate(mat_idx), np.concatenate(mats).astype(np.complex128))
+
+
+@dataclass
+class FlatCircuit:
+    """One circuit as the flat arrays of registry_apply_many / dk_apply_gates."""
+    num_qubits: int
+    op_k: np.ndarray  # uint32 [N]
+    op_targets: np.ndarray  # uint32 [N, 3]
+    op_controls: np.ndarray  # uint64 [N]
+    op_anticontrols: np.ndarray  # uint64 [N]
+    op_matrix: np.ndarray  # uint64 [N]
+    matrices: np.ndarray  # complex128 [M]
+    rolls: np.ndarray
+
+    def arrays(self):
+        return (self.op_k, self.op_targets, self.op_controls, self.op_anticontrols,
+                self.op_matrix, self.matrices)
+
+    @property
+    def count(self) -> int:
+        return int(self.op_k.size)
+
+
+def small_circuit_flat(seed: int = 1, n: int = 12, depth: int = 20) -> FlatCircuit:
+    """small_circuit(seed, n, depth) as flat arrays, drawn from the same
+    seeded stream (three generator calls per layer instead of n + 2, so
+    thousands of circuits can be prepared ahead of a serving run): the gates,
+    qubit choices and rolls are the same; the U3 matrices are computed in
+    one vectorised pass (equal to u3() up to the last bit of the libm
+    functions)."""
+    rng = rng_for(seed)
+    npairs = n // 2
+    per_layer = n + npairs + (1 if n >= 3 else 0)
+    tot = depth * per_layer
+    k = np.ones(tot, dtype=np.uint32)
+    tg = np.zeros((tot, 3), dtype=np.uint32)
+    cm = np.zeros(tot, dtype=np.uint64)
+    am = np.zeros(tot, dtype=np.uint64)
+    mi = np.zeros(tot, dtype=np.uint64)
+    angles = np.empty((depth, n, 3))
+    one = np.uint64(1)
+    for layer in range(depth):
+        angles[layer] = rng.random(3 * n).reshape(n, 3) * 2.0 * np.pi
+        b = layer * per_layer
+        tg[b:b + n, 0] = np.arange(n, dtype=np.uint32)
+        mi[b:b + n] = 4 + 4 * (layer * n + np.arange(n, dtype=np.uint64))
+        perm = rng.permutation(n)
+        p = b + n
+        tg[p:p + npairs, 0] = perm[1:2 * npairs:2]
+        cm[p:p + npairs] = one << perm[0:2 * npairs:2].astype(np.uint64)
+        if n >= 3:
+            t, c, ac = (int(x) for x in rng.choice(n, size=3, replace=False))
+            i = b + n + npairs
+            tg[i, 0] = t
+            cm[i] = one << np.uint64(c)
+            am[i] = one << np.uint64(ac)
+    rolls = rng.random(n)
+    mats = np.concatenate([X.reshape(-1), _u3_many(angles.reshape(-1, 3)).reshape(-1)])
+    return FlatCircuit(n, k, tg, cm, am, mi, mats.astype(np.complex128), rolls)

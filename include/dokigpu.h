@@ -100,6 +100,20 @@ int dk_apply_gate(dk_state *in, const dk_gate *gate, const unsigned *targets,
 		  unsigned num_controls, const unsigned *anticontrols,
 		  unsigned num_anticontrols, dk_state **out);
 
+/* Bulk form of dk_apply_gate (serving form; no counterpart in the
+ * reference, whose callers make one registry_apply call per gate,
+ * doki.c:722-941): queue `count` gates on `in` in order and return the
+ * resulting register.  Gate i acts on op_k[i] <= 3 targets
+ * op_targets[3 i .. 3 i + k - 1] (targets[0] = LSB of the gate index), with
+ * control / anticontrol bit masks op_controls[i] / op_anticontrols[i]; its
+ * 2^k x 2^k row-major complex128 matrix starts at complex entry op_matrix[i]
+ * of `matrices` (num_matrix_entries complex entries in all).  Every gate is
+ * checked before any is queued; count = 0 returns a clone of `in`. */
+int dk_apply_gates(dk_state *in, unsigned count, const unsigned *op_k,
+		   const unsigned *op_targets, const uint64_t *op_controls,
+		   const uint64_t *op_anticontrols, const uint64_t *op_matrix,
+		   const double *matrices, uint64_t num_matrix_entries, dk_state **out);
+
 /* state_get qstate.h:86 (registry_get doki.c:546-595): logical amplitude. */
 int dk_get_amplitude(dk_state *s, uint64_t id, double *re, double *im);
 /* Bulk form of the above: amplitudes [first, first + count) into `out`

@@ -167,3 +167,66 @@ def test_debug_build_checks_stay_clear(dk_gpu, orc, tmp_path, tensor):
             assert np.allclose(got[name + ":" + key], want[key], atol=atol, rtol=0), (name, key)
         assert np.array_equal(got[name + ":mask_results"], want["mask_results"]), name
         assert got[name + ":one_result"][0] == want["one_result"][0], name
+
+
+STARVE = textwrap.dedent("""
+    import ctypes, sys
+    import numpy as np
+    sys.path.insert(0, sys.argv[2])
+    from doki_b200 import workloads as W
+
+    P = ctypes.c_void_p
+    lib = ctypes.CDLL(sys.argv[1])
+    lib.dk_init.argtypes = [ctypes.c_int]
+    lib.dk_gate_new.argtypes = [ctypes.c_uint, P, ctypes.POINTER(P)]
+    lib.dk_gate_free.argtypes = [P]
+    lib.dk_state_new.argtypes = [ctypes.c_uint, ctypes.c_int, ctypes.POINTER(P)]
+    lib.dk_state_free.argtypes = [P]
+    lib.dk_apply_gate.argtypes = [P, P, P, ctypes.c_uint, P, ctypes.c_uint, P, ctypes.c_uint,
+                                  ctypes.POINTER(P)]
+    lib.dk_marginals.argtypes = [P, P]
+    lib.dk_debug_tm_starve.argtypes = [ctypes.c_int]
+
+    def run(n):
+        s = P()
+        assert lib.dk_state_new(n, 1, ctypes.byref(s)) == 0
+        for q in range(n):
+            m = np.ascontiguousarray(W.u3(0.3 + q, 0.2, 0.1), dtype=np.complex128)
+            g = P()
+            assert lib.dk_gate_new(1, m.ctypes.data, ctypes.byref(g)) == 0
+            t = (ctypes.c_uint * 1)(q)
+            o = P()
+            assert lib.dk_apply_gate(s, g, ctypes.cast(t, P), 1, None, 0, None, 0,
+                                     ctypes.byref(o)) == 0
+            lib.dk_state_free(s)
+            lib.dk_gate_free(g)
+            s = o
+        marg = np.empty(n)
+        rc = lib.dk_marginals(s, marg.ctypes.data)
+        lib.dk_state_free(s)
+        return rc, marg
+
+    assert lib.dk_init(0) == 0
+    assert lib.dk_debug_tm_starve(1) == 0
+    rc, _ = run(16)
+    print("starved", rc)
+    assert lib.dk_debug_tm_starve(0) == 0
+    rc2, marg = run(16)
+    print("after", rc2)
+    want = [abs(np.sin((0.3 + q) / 2)) ** 2 for q in range(16)]
+    assert rc2 == 0 and np.allclose(marg, want, atol=1e-6), (rc2, marg)
+    sys.exit(0 if rc == 23 else 3)
+""")
+
+
+def test_tensor_memory_sweep_wait_expires_cleanly(dk_gpu):
+    """Failure detection of the complex64 tcgen05 sweep: with its MMA
+    completions starved (a flag that nothing sets, debug build), each bounded
+    wait expires, the kernel frees its tensor memory and returns, and the
+    read that follows reports DK_ERR_TIMEOUT (23).  The context stays
+    usable: the same circuit run right after is correct."""
+    r = subprocess.run([sys.executable, "-c", STARVE, LIB_DBG, ROOT],
+                       env=dict(os.environ, DK_TENSOR="1"),
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-3000:])
+    assert "starved 23" in r.stdout and "after 0" in r.stdout

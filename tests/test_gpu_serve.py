@@ -103,3 +103,40 @@ def test_join_across_slots_then_reuse_least(dk_gpu, after):
         del b  # b2 alone holds the storage: its sweep runs in place
         d.registry_prob(b2, 0, 1, False)
     assert np.allclose(d.registry_get_all(j, False), np.kron(va, vb), atol=ATOL_C128, rtol=0)
+
+
+def _flat(ops):
+    """ops as the flat arrays registry_apply_many takes."""
+    n = len(ops)
+    k = np.array([op.k for op in ops], dtype=np.uint32)
+    tg = np.zeros((n, 3), dtype=np.uint32)
+    cm = np.zeros(n, dtype=np.uint64)
+    am = np.zeros(n, dtype=np.uint64)
+    mi = np.zeros(n, dtype=np.uint64)
+    mats, off = [], 0
+    for i, op in enumerate(ops):
+        tg[i, :op.k] = op.targets
+        cm[i] = sum(1 << c for c in op.controls)
+        am[i] = sum(1 << c for c in op.anticontrols)
+        mi[i] = off
+        mats.append(np.ascontiguousarray(op.gate, dtype=np.complex128).reshape(-1))
+        off += op.gate.size
+    return k, tg, cm, am, mi, np.concatenate(mats)
+
+
+@pytest.mark.parametrize("precision", [2, 1])
+def test_apply_many_equals_one_call_per_gate(dk_gpu, precision):
+    """registry_apply_many queues the same gates as one registry_apply call
+    per gate: the flushed registers are identical."""
+    d = dk_gpu
+    c = W.small_circuit(seed=44, n=15, depth=6)
+    ops = c.ops + [W.Op(W.u3(0.1, 0.2, 0.3), [3], {7}, {11})]
+    a = W.run_ops(d, d.registry_new(15, False, precision), ops)
+    b = d.registry_apply_many(d.registry_new(15, False, precision), *_flat(ops))
+    assert np.array_equal(d.registry_get_all(a, False), d.registry_get_all(b, False))
+    # rejected as a whole: a target out of range queues nothing
+    bad = list(_flat(ops[:3]))
+    bad[1] = bad[1].copy()
+    bad[1][2, 0] = 15
+    with pytest.raises(d.error):
+        d.registry_apply_many(b, *bad)

@@ -163,3 +163,23 @@ def test_near_tie_collector_keeps_checking_later_trials():
     with pytest.raises(pytest.xfail.Exception, match="trial 1"):
         ties.finish()
     NearTies().finish()  # no near-tie: passes
+
+
+def test_flat_small_circuit_matches_the_op_list():
+    """The vectorised serving-form generator draws the same circuit as
+    small_circuit: same targets, controls, anticontrols and rolls, matrices
+    equal to the last bits of the libm functions."""
+    from doki_b200 import workloads as W
+    for seed, n, depth in ((10_007, 9, 5), (10_012, 2, 3), (10_100, 16, 4)):
+        c = W.small_circuit(seed=seed, n=n, depth=depth)
+        f = W.small_circuit_flat(seed=seed, n=n, depth=depth)
+        assert f.count == len(c.ops)
+        assert np.array_equal(f.rolls, c.rolls)
+        for i, op in enumerate(c.ops):
+            k = int(f.op_k[i])
+            assert k == op.k and list(f.op_targets[i, :k]) == op.targets
+            assert int(f.op_controls[i]) == sum(1 << q for q in op.controls)
+            assert int(f.op_anticontrols[i]) == sum(1 << q for q in op.anticontrols)
+            m0 = int(f.op_matrix[i])
+            mat = f.matrices[m0:m0 + 4].reshape(2, 2)
+            assert np.allclose(mat, op.gate, atol=1e-15, rtol=0)

@@ -7,8 +7,9 @@ once, and every run queues one graph that executes all registers and leaves
 each register's reduced density matrix on the device.
 
 :func:`autotune` is the project's tuner: it times the batch under each
-candidate (tile bits of the streamed registers, CTAs per SM) and caches the
-best choice in a JSON file keyed by device, precision and size histogram.
+candidate (dense-block fusion of the plan, tile bits of the streamed
+registers, CTAs per SM) and caches the best choice in a JSON file keyed by
+device, precision and size histogram.
 """
 from __future__ import annotations
 
@@ -36,7 +37,7 @@ def lib() -> ctypes.CDLL:
         L = ctypes.CDLL(os.path.join(_HERE, "libdokigpu.so"))
         L.dk_batch_build.argtypes = [ctypes.c_int, ctypes.c_uint, _u32p, _u32p, _u64p, _u32p,
                                      _u32p, _u64p, _u64p, _u64p, _dp, ctypes.c_int,
-                                     ctypes.POINTER(ctypes.c_void_p)]
+                                     ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
         L.dk_batch_build.restype = ctypes.c_int
         L.dk_batch_set_ctas.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.dk_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -48,6 +49,7 @@ def lib() -> ctypes.CDLL:
         L.dk_batch_rho_elems.argtypes = [ctypes.c_void_p]
         L.dk_batch_rho_elems.restype = ctypes.c_uint64
         L.dk_batch_state.argtypes = [ctypes.c_void_p, ctypes.c_uint, _dp]
+        L.dk_batch_compare.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _dp, _dp]
         L.dk_batch_error.argtypes = [ctypes.c_void_p]
         L.dk_batch_error.restype = ctypes.c_char_p
         L.dk_batch_free.argtypes = [ctypes.c_void_p]
@@ -69,7 +71,7 @@ class BatchEngine:
     """A planned, device-resident batch of circuits."""
 
     def __init__(self, batch: FlatBatch, precision: int = 1, tile_bits: int = 12,
-                 ctas_per_sm: int = 1):
+                 ctas_per_sm: int = 1, fold: int = 0):
         L = lib()
         self.batch = batch
         self.precision = precision
@@ -86,11 +88,13 @@ class BatchEngine:
         rc = L.dk_batch_build(precision, batch.count, _ptr(nq, _u32p), _ptr(keep, _u32p),
                               _ptr(st, _u64p), _ptr(k, _u32p), _ptr(tg, _u32p),
                               _ptr(cm, _u64p), _ptr(am, _u64p), _ptr(mi, _u64p),
-                              _ptr(mats.view(np.float64), _dp), tile_bits, ctypes.byref(h))
+                              _ptr(mats.view(np.float64), _dp), tile_bits, fold,
+                              ctypes.byref(h))
         if rc:
             raise BatchError(f"dk_batch_build: {L.dk_strerror(rc).decode()}")
         self._h = h
         self.tile_bits = tile_bits
+        self.fold = fold
         if ctas_per_sm != 1:
             self.set_ctas(ctas_per_sm)
         self.ctas_per_sm = ctas_per_sm
@@ -136,6 +140,16 @@ class BatchEngine:
                     "dk_batch_state")
         return out
 
+    def compare(self, other: "BatchEngine") -> Tuple[np.ndarray, np.ndarray]:
+        """Per-circuit fidelity and largest amplitude difference of this
+        batch's final registers against `other`'s (same circuits; both run
+        with keep_states), computed on the device in FP64."""
+        fid = np.empty(self.batch.count)
+        err = np.empty(self.batch.count)
+        self._check(lib().dk_batch_compare(self._h, other._h, _ptr(fid, _dp), _ptr(err, _dp)),
+                    "dk_batch_compare")
+        return fid, err
+
     def close(self):
         if getattr(self, "_h", None):
             lib().dk_batch_free(self._h)
@@ -172,10 +186,13 @@ def default_cache_path() -> str:
 
 
 def autotune(batch: FlatBatch, precision: int, tile_bits: Iterable[int] = (10, 11, 12),
-             ctas: Iterable[int] = (1, 2), reps: int = 2,
+             ctas: Iterable[int] = (1, 2), folds: Iterable[int] = (-1, 0, 400), reps: int = 2,
              cache_path: Optional[str] = None, device_name: str = "") -> Dict:
-    """Pick tile bits (streamed registers) and CTAs per SM by timing the batch;
-    results are cached per (device, precision, batch signature)."""
+    """Pick the dense-block fusion of the plan (`fold`: -1 every gate on its
+    own, 0 the planner's default, larger values fold runs of gates into 8x8
+    products more readily), tile bits (streamed registers) and CTAs per SM
+    by timing the batch under every combination; results, with every trial,
+    are cached per (device, precision, batch signature)."""
     path = cache_path or default_cache_path()
     key = f"{device_name}|{_signature(batch, precision)}"
     try:
@@ -183,18 +200,20 @@ def autotune(batch: FlatBatch, precision: int, tile_bits: Iterable[int] = (10, 1
             cache = json.load(f)
     except (OSError, ValueError):
         cache = {}
-    if key in cache:
+    if key in cache and "fold" in cache[key]:
         return dict(cache[key], cached=True)
     trials = []
-    for tb in tile_bits:
-        eng = BatchEngine(batch, precision, tile_bits=tb)
-        for c in ctas:
-            eng.set_ctas(c)
-            trials.append({"tile_bits": tb, "ctas_per_sm": c, "seconds": time_runs(eng, reps)})
-        eng.close()
+    for fold in folds:
+        for tb in tile_bits:
+            eng = BatchEngine(batch, precision, tile_bits=tb, fold=fold)
+            for c in ctas:
+                eng.set_ctas(c)
+                trials.append({"fold": fold, "tile_bits": tb, "ctas_per_sm": c,
+                               "seconds": time_runs(eng, reps)})
+            eng.close()
     best = min(trials, key=lambda t: t["seconds"])
-    result = {"tile_bits": best["tile_bits"], "ctas_per_sm": best["ctas_per_sm"],
-              "seconds": best["seconds"], "trials": trials}
+    result = {"fold": best["fold"], "tile_bits": best["tile_bits"],
+              "ctas_per_sm": best["ctas_per_sm"], "seconds": best["seconds"], "trials": trials}
     cache[key] = result
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)

@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "dk_device.cuh"
@@ -227,6 +228,60 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
 	}
 }
 
+/* Per-register comparison of two batches of the same circuits (precision
+ * form of the batch): fidelity |<x|y>|^2 / (<x|x> <y|y>) and the largest
+ * |x_i / |x| - y_i / |y||, in FP64, one CTA per register (states in each
+ * batch's own layout and precision; both offset tables are the same). */
+template <typename CX, typename CY>
+__global__ void __launch_bounds__(256)
+	k_batch_compare(const CX *__restrict__ xs, const CY *__restrict__ ys,
+			const uint64_t *__restrict__ offs, const uint32_t *__restrict__ ns,
+			double *fid, double *err)
+{
+	const unsigned c = blockIdx.x;
+	const uint64_t o = offs[c], cnt = 1ull << ns[c];
+	double xr = 0.0, xi = 0.0, xx = 0.0, yy = 0.0;
+	for (uint64_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+		const double2 x = to_c128(xs[o + i]), y = to_c128(ys[o + i]);
+		xr += x.x * y.x + x.y * y.y; /* conj(x) y */
+		xi += x.x * y.y - x.y * y.x;
+		xx += sqabs(x);
+		yy += sqabs(y);
+	}
+	__shared__ double red[4][256];
+	red[0][threadIdx.x] = xr;
+	red[1][threadIdx.x] = xi;
+	red[2][threadIdx.x] = xx;
+	red[3][threadIdx.x] = yy;
+	__syncthreads();
+	for (int st = blockDim.x >> 1; st > 0; st >>= 1) {
+		if ((int)threadIdx.x < st)
+			for (int k = 0; k < 4; ++k)
+				red[k][threadIdx.x] += red[k][threadIdx.x + st];
+		__syncthreads();
+	}
+	const double sx = 1.0 / sqrt(red[2][0]), sy = 1.0 / sqrt(red[3][0]);
+	if (threadIdx.x == 0)
+		fid[c] = (red[0][0] * red[0][0] + red[1][0] * red[1][0]) / (red[2][0] * red[3][0]);
+	double m = 0.0;
+	for (uint64_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+		const double2 x = to_c128(xs[o + i]), y = to_c128(ys[o + i]);
+		const double dr = x.x * sx - y.x * sy, di = x.y * sx - y.y * sy;
+		m = fmax(m, sqrt(dr * dr + di * di));
+	}
+	__syncthreads();
+	red[0][threadIdx.x] = m;
+	__syncthreads();
+	for (int st = blockDim.x >> 1; st > 0; st >>= 1) {
+		if ((int)threadIdx.x < st)
+			red[0][threadIdx.x] = fmax(red[0][threadIdx.x], red[0][threadIdx.x + st]);
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) {
+		err[c] = red[0][0];
+	}
+}
+
 } // namespace
 } // namespace dk
 
@@ -307,7 +362,7 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 		   const unsigned *keep_qubits, const uint64_t *op_start, const unsigned *op_k,
 		   const unsigned *op_targets, const uint64_t *op_controls,
 		   const uint64_t *op_anticontrols, const uint64_t *op_matrix,
-		   const double *matrices, int tile_bits, dk_batch **out)
+		   const double *matrices, int tile_bits, int fold, dk_batch **out)
 {
 	DK_TRACE();
 	if (!out || (precision != DK_C64 && precision != DK_C128) || !num_qubits ||
@@ -315,6 +370,15 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 		return DK_ERR_ARG;
 	if (tile_bits < 8 || tile_bits > 12)
 		return DK_ERR_ARG;
+	for (unsigned c = 0; c < num_circuits; ++c) {
+		const unsigned n = num_qubits[c];
+		if (n < 4 || n > 16 || keep_qubits[c] > n || keep_qubits[c] > 12 ||
+		    op_start[c + 1] < op_start[c])
+			return DK_ERR_ARG;
+		for (uint64_t i = op_start[c]; i < op_start[c + 1]; ++i)
+			if (op_k[i] == 0 || op_k[i] > 3)
+				return DK_ERR_ARG;
+	}
 	int rc = dk_init(-1);
 	if (rc)
 		return rc;
@@ -322,7 +386,6 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 	b->prec = precision;
 	b->tile_bits = tile_bits;
 	b->ncirc = num_circuits;
-	cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, 0);
 	{
 		int dev = 0;
 		cudaGetDevice(&dev);
@@ -335,78 +398,110 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 	b->state_off.resize(num_circuits);
 	b->n.assign(num_qubits, num_qubits + num_circuits);
 	b->keep.assign(keep_qubits, keep_qubits + num_circuits);
-	std::vector<dk_gate> gates;
-	std::vector<dk_flat_op> flat;
-	for (unsigned c = 0; c < num_circuits; ++c) {
-		const unsigned n = num_qubits[c];
-		const unsigned keep = keep_qubits[c];
-		if (n < 4 || n > 16 || keep > n || keep > 12) {
-			delete b;
-			return DK_ERR_ARG;
-		}
-		const uint64_t o0 = op_start[c], o1 = op_start[c + 1];
-		gates.resize(o1 - o0);
-		flat.resize(o1 - o0);
-		for (uint64_t i = o0; i < o1; ++i) {
-			dk_gate &gt = gates[i - o0];
-			gt.refcount = 1;
-			gt.k = op_k[i];
-			gt.dim = 1ull << gt.k;
-			gt.m = const_cast<double *>(matrices + 2 * op_matrix[i]);
-			dk_flat_op &f = flat[i - o0];
-			memset(&f, 0, sizeof(f));
-			f.gate = &gt;
-			f.k = gt.k;
-			for (unsigned j = 0; j < gt.k && j < 3; ++j)
-				f.tg[j] = op_targets[3 * i + j];
-			f.cm = op_controls[i];
-			f.am = op_anticontrols[i];
-			if (gt.k == 0 || gt.k > 3) {
-				delete b;
-				return DK_ERR_ARG;
+
+	/* Plan every circuit on its own (the planner is reentrant), on all host
+	 * cores: circuit c goes to worker c mod T.  Each circuit's sweep
+	 * programs are kept back to back in its own byte vector. */
+	struct Planned {
+		std::vector<unsigned char> prog;
+		uint32_t nsweep = 0;
+		int rc = 0;
+	};
+	std::vector<Planned> planned(num_circuits);
+	auto plan_some = [&](unsigned first, unsigned stride) {
+		std::vector<dk_gate> gates;
+		std::vector<dk_flat_op> flat;
+		for (unsigned c = first; c < num_circuits; c += stride) {
+			Planned &pl = planned[c];
+			const unsigned n = num_qubits[c];
+			const uint64_t o0 = op_start[c], o1 = op_start[c + 1];
+			gates.resize(o1 - o0);
+			flat.resize(o1 - o0);
+			for (uint64_t i = o0; i < o1; ++i) {
+				dk_gate &gt = gates[i - o0];
+				gt.refcount = 1;
+				gt.k = op_k[i];
+				gt.dim = 1ull << gt.k;
+				gt.m = const_cast<double *>(matrices + 2 * op_matrix[i]);
+				dk_flat_op &f = flat[i - o0];
+				memset(&f, 0, sizeof(f));
+				f.gate = &gt;
+				f.k = gt.k;
+				for (unsigned j = 0; j < gt.k && j < 3; ++j)
+					f.tg[j] = op_targets[3 * i + j];
+				f.cm = op_controls[i];
+				f.am = op_anticontrols[i];
 			}
+			const int m = n <= 12 ? (int)n : tile_bits;
+			dk_plan_limits lim = {};
+			lim.tile_bits = m;
+			lim.tensor = -1; /* the batch kernel runs scalar passes */
+			lim.fold = fold;
+			dk_plan_default_limits(precision, n, &lim);
+			lim.tile_bits = m;
+			if (lim.low_bits > m - 3)
+				lim.low_bits = m - 3;
+			dk_plan plan;
+			pl.rc = dk_plan_build(flat.data(), (int)flat.size(), n, precision, &lim, &plan);
+			if (pl.rc)
+				continue;
+			for (int st = 0; st < plan.nsteps && !pl.rc; ++st) {
+				if (plan.steps[st].kind != 1) {
+					pl.rc = DK_ERR_ARG; /* batches run sweepable gates only */
+					break;
+				}
+				const dk_sweep_hdr *h =
+					(const dk_sweep_hdr *)(plan.blob + plan.steps[st].prog_off);
+				const size_t at = pl.prog.size();
+				pl.prog.resize(at + h->bytes);
+				memcpy(pl.prog.data() + at, h, h->bytes);
+				if (precision == DK_C64) {
+					/* store the matrices in the amplitude precision, in place */
+					dk_sweep_hdr *hh = (dk_sweep_hdr *)(pl.prog.data() + at);
+					const double *src =
+						(const double *)(pl.prog.data() + at + hh->mat_off);
+					float *dst = (float *)(pl.prog.data() + at + hh->mat_off);
+					const size_t nv = 2 * ((hh->bytes - hh->mat_off) / 16);
+					for (size_t v = 0; v < nv; ++v)
+						dst[v] = (float)src[v];
+				}
+			}
+			pl.nsweep = (uint32_t)plan.nsteps;
+			dk_plan_free(&plan);
 		}
-		const int m = n <= 12 ? (int)n : tile_bits;
-		dk_plan_limits lim = {};
-		lim.tile_bits = m;
-		lim.tensor = -1; /* the batch kernel runs scalar passes */
-		dk_plan_default_limits(precision, n, &lim);
-		lim.tile_bits = m;
-		if (lim.low_bits > m - 3)
-			lim.low_bits = m - 3;
-		dk_plan plan;
-		rc = dk_plan_build(flat.data(), (int)flat.size(), n, precision, &lim, &plan);
-		if (rc) {
+	};
+	unsigned T = std::thread::hardware_concurrency();
+	if (T == 0)
+		T = 1;
+	if (T > 64)
+		T = 64;
+	if (T > num_circuits)
+		T = num_circuits;
+	{
+		std::vector<std::thread> pool;
+		for (unsigned t = 1; t < T; ++t)
+			pool.emplace_back(plan_some, t, T);
+		plan_some(0, T);
+		for (auto &th : pool)
+			th.join();
+	}
+	for (unsigned c = 0; c < num_circuits; ++c) {
+		if (planned[c].rc) {
+			rc = planned[c].rc;
 			delete b;
 			return rc;
 		}
+		const unsigned n = num_qubits[c];
+		const unsigned keep = keep_qubits[c];
+		const int m = n <= 12 ? (int)n : tile_bits;
 		dk_breg reg;
 		memset(&reg, 0, sizeof(reg));
-		size_t start = (blob.size() + 15) & ~(size_t)15;
+		const size_t start = (blob.size() + 15) & ~(size_t)15;
 		blob.resize(start);
 		reg.prog = start;
-		for (int s = 0; s < plan.nsteps; ++s) {
-			if (plan.steps[s].kind != 1) {
-				dk_plan_free(&plan);
-				delete b;
-				return DK_ERR_ARG; /* batches run sweepable gates only */
-			}
-			const dk_sweep_hdr *h = (const dk_sweep_hdr *)(plan.blob + plan.steps[s].prog_off);
-			size_t at = blob.size();
-			blob.resize(at + h->bytes);
-			memcpy(blob.data() + at, h, h->bytes);
-			if (precision == DK_C64) {
-				/* store the matrices in the amplitude precision, in place */
-				dk_sweep_hdr *hh = (dk_sweep_hdr *)(blob.data() + at);
-				const double *src = (const double *)(blob.data() + at + hh->mat_off);
-				float *dst = (float *)(blob.data() + at + hh->mat_off);
-				const size_t nv = 2 * ((hh->bytes - hh->mat_off) / 16);
-				for (size_t v = 0; v < nv; ++v)
-					dst[v] = (float)src[v];
-			}
-		}
-		reg.nsweep = (uint32_t)plan.nsteps;
-		dk_plan_free(&plan);
+		blob.insert(blob.end(), planned[c].prog.begin(), planned[c].prog.end());
+		std::vector<unsigned char>().swap(planned[c].prog);
+		reg.nsweep = planned[c].nsweep;
 		reg.n = n;
 		reg.keep = keep;
 		reg.state = b->state_amps;
@@ -636,6 +731,66 @@ int dk_batch_state(dk_batch *b, unsigned circuit, double *out)
 		for (size_t i = 0; i < 2 * cnt; ++i)
 			out[i] = f[i];
 	}
+	return DK_OK;
+}
+
+int dk_batch_compare(dk_batch *x, dk_batch *y, double *fidelity, double *max_amp_err)
+{
+	DK_TRACE();
+	if (!x || !y || !fidelity || !max_amp_err || x->ncirc != y->ncirc || x->n != y->n ||
+	    !x->dstates || !y->dstates)
+		return DK_ERR_ARG;
+	const unsigned nc = x->ncirc;
+	/* both batches' work is done before the comparison reads them */
+	cudaError_t e = cudaStreamSynchronize(y->st);
+	uint64_t *doffs = nullptr;
+	uint32_t *dns = nullptr;
+	double *dout = nullptr;
+	if (e == cudaSuccess)
+		e = cudaMallocAsync(&doffs, sizeof(uint64_t) * nc, x->st);
+	if (e == cudaSuccess)
+		e = cudaMallocAsync(&dns, sizeof(uint32_t) * nc, x->st);
+	if (e == cudaSuccess)
+		e = cudaMallocAsync(&dout, 2 * sizeof(double) * nc, x->st);
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(doffs, x->state_off.data(), sizeof(uint64_t) * nc,
+				    cudaMemcpyHostToDevice, x->st);
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(dns, x->n.data(), sizeof(uint32_t) * nc, cudaMemcpyHostToDevice,
+				    x->st);
+	if (e == cudaSuccess) {
+		if (x->prec == DK_C64 && y->prec == DK_C128)
+			dk::k_batch_compare<float2, double2><<<nc, 256, 0, x->st>>>(
+				(const float2 *)x->dstates, (const double2 *)y->dstates, doffs, dns,
+				dout, dout + nc);
+		else if (x->prec == DK_C128 && y->prec == DK_C64)
+			dk::k_batch_compare<double2, float2><<<nc, 256, 0, x->st>>>(
+				(const double2 *)x->dstates, (const float2 *)y->dstates, doffs, dns,
+				dout, dout + nc);
+		else if (x->prec == DK_C64)
+			dk::k_batch_compare<float2, float2><<<nc, 256, 0, x->st>>>(
+				(const float2 *)x->dstates, (const float2 *)y->dstates, doffs, dns, dout,
+				dout + nc);
+		else
+			dk::k_batch_compare<double2, double2><<<nc, 256, 0, x->st>>>(
+				(const double2 *)x->dstates, (const double2 *)y->dstates, doffs, dns,
+				dout, dout + nc);
+		e = cudaGetLastError();
+		dk::g_launches += 1;
+	}
+	std::vector<double> host(2 * (size_t)nc);
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(host.data(), dout, 2 * sizeof(double) * nc,
+				    cudaMemcpyDeviceToHost, x->st);
+	cudaFreeAsync(doffs, x->st);
+	cudaFreeAsync(dns, x->st);
+	cudaFreeAsync(dout, x->st);
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(x->st);
+	if (e != cudaSuccess)
+		return batch_cuda_fail(x, e);
+	memcpy(fidelity, host.data(), sizeof(double) * nc);
+	memcpy(max_amp_err, host.data() + nc, sizeof(double) * nc);
 	return DK_OK;
 }
 

@@ -1300,6 +1300,55 @@ __global__ void __launch_bounds__(256)
 	}
 }
 
+/* Half of a register for an exchange between ranks (distributed registers):
+ * dst[j] = scale * in[i(j)], i(j) = j with `value` inserted at bit `bit`,
+ * for the 2^(n-1) indices j in order. */
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_read_half(const typename CT<R>::T *__restrict__ in, uint64_t half, unsigned bit,
+		    int value, double scale, typename CT<R>::T *dst)
+{
+	typedef typename CT<R>::T C2;
+	const uint64_t low = (1ull << bit) - 1ull;
+	for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < half;
+	     j += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t i = ((j & ~low) << 1) | ((uint64_t)value << bit) | (j & low);
+		const double2 v = to_c128(in[i]);
+		dst[j] = from_c128<C2>(make_double2(v.x * scale, v.y * scale));
+	}
+}
+
+/* The register with its half at bit `bit` = `value` replaced:
+ * out[i] = src[j(i)] there (j(i) = i with bit `bit` removed), scale * in[i]
+ * elsewhere; per-block sums of |out|^2 for the new register's scalars. */
+template <typename R>
+__global__ void __launch_bounds__(256)
+	k_replace_half(const typename CT<R>::T *__restrict__ in,
+		       const typename CT<R>::T *__restrict__ src, uint64_t size, unsigned bit,
+		       int value, double scale, typename CT<R>::T *out, double *partials)
+{
+	typedef typename CT<R>::T C2;
+	const uint64_t low = (1ull << bit) - 1ull;
+	double sq = 0.0, dummy = 0.0;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < size;
+	     i += (uint64_t)gridDim.x * blockDim.x) {
+		C2 v;
+		if ((int)((i >> bit) & 1ull) == value) {
+			v = src[((i >> 1) & ~low) | (i & low)];
+		} else {
+			const double2 x = to_c128(in[i]);
+			v = from_c128<C2>(make_double2(x.x * scale, x.y * scale));
+		}
+		out[i] = v;
+		sq += sqabs(v);
+	}
+	block_sum2(dummy, sq);
+	if (threadIdx.x == 0) {
+		partials[2 * blockIdx.x] = 0.0;
+		partials[2 * blockIdx.x + 1] = sq;
+	}
+}
+
 __global__ void k_clear_flags(dk_scal *sc)
 {
 	sc->zero_norm = 0;
@@ -2347,6 +2396,42 @@ cudaError_t launch_import(int prec, const double *src, void *d, unsigned n,
 	else
 		k_import<float><<<blocks, 256, 0, st>>>((const double2 *)src,
 						       (float2 *)d, size, s.partials);
+	k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc, sc, FIN_RESET, 1);
+	g_launches += 3;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_read_half(int prec, const void *in, unsigned n, unsigned bit, int value,
+			     double scale, void *dst, cudaStream_t st)
+{
+	const uint64_t half = 1ull << (n - 1);
+	const int blocks = grid_for(half, 256 * 4, g_num_sms * 8);
+	if (prec == DK_C128)
+		k_read_half<double><<<blocks, 256, 0, st>>>((const double2 *)in, half, bit, value,
+							    scale, (double2 *)dst);
+	else
+		k_read_half<float><<<blocks, 256, 0, st>>>((const float2 *)in, half, bit, value,
+							   scale, (float2 *)dst);
+	g_launches += 1;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_replace_half(int prec, const void *in, const void *src, unsigned n,
+				unsigned bit, int value, double scale, void *out, dk_scal *sc,
+				const Scratch &s, cudaStream_t st)
+{
+	const uint64_t size = 1ull << n;
+	const int blocks = grid_for(size, 256 * 4, g_num_sms * 8);
+	k_clear_flags<<<1, 1, 0, st>>>(sc);
+	if (prec == DK_C128)
+		k_replace_half<double><<<blocks, 256, 0, st>>>((const double2 *)in,
+							       (const double2 *)src, size, bit,
+							       value, scale, (double2 *)out,
+							       s.partials);
+	else
+		k_replace_half<float><<<blocks, 256, 0, st>>>((const float2 *)in, (const float2 *)src,
+							      size, bit, value, scale, (float2 *)out,
+							      s.partials);
 	k_finalize<<<1, 256, 0, st>>>(s.partials, blocks, sc, sc, FIN_RESET, 1);
 	g_launches += 3;
 	return cudaGetLastError();

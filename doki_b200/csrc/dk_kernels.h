@@ -49,6 +49,16 @@ cudaError_t launch_generic_gate(int prec, const void *in, void *out,
 				const dk_scal *sc_in, dk_scal *sc_out,
 				const Scratch &s, cudaStream_t st);
 
+/* distributed registers: scale x the half of `in` (raw amplitudes) at
+ * bit = value into dst (2^(n-1), storage precision) */
+cudaError_t launch_read_half(int prec, const void *in, unsigned n, unsigned bit, int value,
+			     double scale, void *dst, cudaStream_t st);
+/* out = in with its half at bit = value taken from src and the rest scaled
+ * by `scale`; out's scalars: csq = sum |out|^2, norm = 1 */
+cudaError_t launch_replace_half(int prec, const void *in, const void *src, unsigned n,
+				unsigned bit, int value, double scale, void *out, dk_scal *sc,
+				const Scratch &s, cudaStream_t st);
+
 /* |0..0>: zero + amp[0] = 1, norm = csq = 1 */
 cudaError_t launch_init_zero(int prec, void *d, unsigned n, dk_scal *sc,
 			     cudaStream_t st);

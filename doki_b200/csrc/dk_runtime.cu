@@ -900,6 +900,102 @@ int dk_apply_gates(dk_state *in, unsigned count, const unsigned *op_k,
 	return DK_OK;
 }
 
+int dk_state_norm(dk_state *s, double *norm, double *stored_norm)
+{
+	DK_TRACE();
+	SlotLock lk(s ? s->slot : t_slot);
+	int rc = prepare_read(s);
+	if (rc)
+		return rc;
+	if (!norm || !stored_norm)
+		return DK_ERR_ARG;
+	*norm = s->norm;
+	*stored_norm = sqrt(s->csq);
+	return DK_OK;
+}
+
+int dk_state_read_half(dk_state *s, unsigned bit, int value, double scale, void *dst,
+		       int on_device)
+{
+	DK_TRACE();
+	SlotLock lk(s ? s->slot : t_slot);
+	int rc = prepare_read(s);
+	if (rc)
+		return rc;
+	if (!dst || bit >= s->n || (value != 0 && value != 1))
+		return DK_ERR_ARG;
+	const size_t bytes = amp_bytes(s->prec) << (s->n - 1);
+	void *target = dst;
+	if (!on_device) {
+		rc = dev_alloc(&target, bytes);
+		if (rc)
+			return rc;
+	}
+	/* logical = stored / norm */
+	cudaError_t e = dk::launch_read_half(s->prec, s->buf->d, s->n, bit, value,
+					     scale / s->norm, target, CUR.st);
+	if (!on_device) {
+		if (e == cudaSuccess)
+			e = cudaMemcpyAsync(dst, target, bytes, cudaMemcpyDeviceToHost, CUR.st);
+		g.d2h += bytes;
+		dev_free(target, bytes);
+	}
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(CUR.st);
+	return e == cudaSuccess ? DK_OK : cuda_fail(e);
+}
+
+int dk_state_replace_half(dk_state *in, unsigned bit, int value, double scale, const void *src,
+			  int on_device, dk_state **out)
+{
+	DK_TRACE();
+	SlotLock lk(in ? in->slot : t_slot);
+	int rc = prepare_read(in);
+	if (rc)
+		return rc;
+	if (!src || !out || bit >= in->n || (value != 0 && value != 1))
+		return DK_ERR_ARG;
+	const size_t bytes = amp_bytes(in->prec) << (in->n - 1);
+	dk_state *s = state_alloc(in->n, in->prec, in->slot);
+	if (!s)
+		return DK_ERR_ALLOC;
+	rc = buf_new(in->n, in->prec, &s->buf);
+	if (rc) {
+		free(s);
+		return rc;
+	}
+	const void *from = src;
+	void *stage = nullptr;
+	cudaError_t e = cudaSuccess;
+	if (!on_device) {
+		rc = dev_alloc(&stage, bytes);
+		if (rc) {
+			dk_state_free(s);
+			return rc;
+		}
+		e = cudaMemcpyAsync(stage, src, bytes, cudaMemcpyHostToDevice, CUR.st);
+		g.h2d += bytes;
+		from = stage;
+	}
+	if (e == cudaSuccess)
+		e = dk::launch_replace_half(in->prec, in->buf->d, from, in->n, bit, value,
+					    scale / in->norm, s->buf->d, s->buf->sc, CUR.scratch,
+					    CUR.st);
+	if (stage) {
+		/* pageable source: the copy is staged before cudaMemcpyAsync
+		 * returns; the kernel reads the device stage before the free */
+		dev_free(stage, bytes);
+	}
+	if (e == cudaSuccess && !on_device)
+		e = cudaStreamSynchronize(CUR.st);
+	if (e != cudaSuccess) {
+		dk_state_free(s);
+		return cuda_fail(e);
+	}
+	*out = s;
+	return DK_OK;
+}
+
 int dk_get_amplitude(dk_state *s, uint64_t id, double *re, double *im)
 {
 	DK_TRACE();

@@ -1131,6 +1131,70 @@ r1:
 	return res;
 }
 
+/* Distributed registers' local view (dk_state_norm / read_half /
+ * replace_half): pointers are integers (numpy .ctypes.data, a torch
+ * tensor's data_ptr()), in the register's storage precision. */
+static PyObject *doki_registry_norm(PyObject *self, PyObject *args)
+{
+	PyObject *cap;
+	if (!PyArg_ParseTuple(args, "O", &cap)) {
+		PyErr_SetString(DokiError, "Syntax: registry_norm(registry)");
+		return NULL;
+	}
+	dk_state *s = get_state(cap, "NULL pointer to registry");
+	if (!s)
+		return NULL;
+	double nrm = 0.0, stored = 0.0;
+	int rc;
+	Py_BEGIN_ALLOW_THREADS rc = dk_state_norm(s, &nrm, &stored);
+	Py_END_ALLOW_THREADS if (rc) return raise_dk(rc, "Failed to read the norm");
+	return Py_BuildValue("(dd)", nrm, stored);
+}
+
+static PyObject *doki_registry_read_half(PyObject *self, PyObject *args)
+{
+	PyObject *cap;
+	unsigned bit;
+	int value, on_device;
+	double scale;
+	unsigned long long ptr;
+	if (!PyArg_ParseTuple(args, "OIidKp", &cap, &bit, &value, &scale, &ptr, &on_device)) {
+		PyErr_SetString(DokiError, "Syntax: registry_read_half(registry, bit, value, scale, "
+					   "dst_pointer, on_device)");
+		return NULL;
+	}
+	dk_state *s = get_state(cap, "NULL pointer to registry");
+	if (!s)
+		return NULL;
+	int rc;
+	Py_BEGIN_ALLOW_THREADS rc = dk_state_read_half(s, bit, value, scale, (void *)ptr, on_device);
+	Py_END_ALLOW_THREADS if (rc) return raise_dk(rc, "Failed to read half of the registry");
+	Py_RETURN_NONE;
+}
+
+static PyObject *doki_registry_replace_half(PyObject *self, PyObject *args)
+{
+	PyObject *cap;
+	unsigned bit;
+	int value, on_device;
+	double scale;
+	unsigned long long ptr;
+	if (!PyArg_ParseTuple(args, "OIidKp", &cap, &bit, &value, &scale, &ptr, &on_device)) {
+		PyErr_SetString(DokiError, "Syntax: registry_replace_half(registry, bit, value, "
+					   "scale, src_pointer, on_device)");
+		return NULL;
+	}
+	dk_state *s = get_state(cap, "NULL pointer to registry");
+	if (!s)
+		return NULL;
+	dk_state *out = NULL;
+	int rc;
+	Py_BEGIN_ALLOW_THREADS rc = dk_state_replace_half(s, bit, value, scale, (const void *)ptr,
+							   on_device, &out);
+	Py_END_ALLOW_THREADS if (rc) return raise_dk(rc, "Failed to replace half of the registry");
+	return wrap_state(out);
+}
+
 static PyObject *doki_registry_join(PyObject *self, PyObject *args)
 {
 	PyObject *c1, *c2;
@@ -2296,6 +2360,12 @@ static PyMethodDef DokiMethods[] = {
 	  "Functional column vector after applying a gate to a functional state" },
 	{ "funmatrix_mem", doki_funmatrix_mem, METH_VARARGS,
 	  "Get the memory allocated by this FMatrix in bytes" },
+	{ "registry_norm", doki_registry_norm, METH_VARARGS,
+	  "(norm constant, 2-norm of the stored amplitudes) of a registry" },
+	{ "registry_read_half", doki_registry_read_half, METH_VARARGS,
+	  "Copy scale x the half of a registry at bit = value (distributed registers)" },
+	{ "registry_replace_half", doki_registry_replace_half, METH_VARARGS,
+	  "New registry with its half at bit = value replaced (distributed registers)" },
 	{ "registry_apply_many", doki_registry_apply_many, METH_VARARGS,
 	  "Queue every gate of a circuit given as flat arrays (serving form)" },
 	{ "registry_get_all", doki_registry_get_all, METH_VARARGS,

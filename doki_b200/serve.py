@@ -5,14 +5,20 @@ Requests arrive as a Poisson stream.  Each carries a circuit of n qubits
 from the plain method's CPU-runnable generator (U3 on every qubit, CNOT on a
 random pairing, one Toffoli with an anticontrol per layer), and a terminal
 operation: all single-qubit probabilities, or the measurement of k in [1, 8]
-random qubits with seeded draws.
+random qubits with seeded draws.  A request arrives with its circuit as
+data (the flat gate arrays of ``registry_apply_many``, built by the client
+before the stream starts: :func:`prepare`), as a request to a server does.
 
 The server keeps `workers` requests in flight, each on its own stream slot of
 the engine (so their kernels overlap on the device), admits the next request
 in arrival order as soon as a slot is free and its register fits in the HBM
-budget, keeps every register resident on the device from its first gate to
-its result, and records per-request latency from arrival to result on the
-host.  `workers=1` with no overlap is the plain one-at-a-time path.
+budget, queues the whole circuit with one ``registry_apply_many`` call (no
+Python work per gate, the interpreter lock released), keeps every register
+resident on the device from its first gate to its result, and records
+per-request latency from arrival to result on the host.
+
+The plain path (:func:`run_plain`) is the reference's way of using the
+module: one request at a time, one ``registry_apply`` call per gate.
 """
 from __future__ import annotations
 
@@ -39,6 +45,14 @@ class Request:
 
     def circuit(self) -> W.Circuit:
         return W.small_circuit(seed=self.seed, n=self.n, depth=self.depth)
+
+    def flat(self) -> W.FlatCircuit:
+        """The circuit as flat gate arrays (built once, kept)."""
+        f = self.__dict__.get("_flat")
+        if f is None:
+            f = W.small_circuit_flat(seed=self.seed, n=self.n, depth=self.depth)
+            self.__dict__["_flat"] = f
+        return f
 
     def state_bytes(self, precision: int) -> int:
         return (16 if precision == 2 else 8) << self.n
@@ -74,18 +88,70 @@ def with_rate(reqs: Sequence[Request], rate: float, seed: int = 6) -> List[Reque
     rng = W.rng_for(seed)
     gaps = rng.exponential(1.0 / rate, size=len(reqs))
     arr = np.cumsum(gaps) - gaps[0]
-    return [Request(r.rid, float(a), r.n, r.depth, r.seed, r.terminal, r.mask, r.rolls)
-            for r, a in zip(reqs, arr)]
+    out = []
+    for r, a in zip(reqs, arr):
+        q = Request(r.rid, float(a), r.n, r.depth, r.seed, r.terminal, r.mask, r.rolls)
+        if "_flat" in r.__dict__:  # keep the prepared circuit
+            q.__dict__["_flat"] = r.__dict__["_flat"]
+        out.append(q)
+    return out
 
 
-def execute(d, req: Request, precision: int):
-    """Run one request through the doki API on the calling thread's slot."""
-    c = req.circuit()
-    reg = W.run_ops(d, d.registry_new(req.n, False, precision), c.ops)
+def prepare(reqs: Sequence[Request]) -> None:
+    """Build every request's circuit arrays ahead of the stream (the
+    client's work, outside any timed run)."""
+    for r in reqs:
+        r.flat()
+
+
+def _terminal(d, reg, req: Request):
     if req.terminal == "probs":
         return ("probs", d.registry_probs(reg))
     _, res = d.registry_measure(reg, req.mask, req.rolls, -1, False)
     return ("measure", res)
+
+
+def execute(d, req: Request, precision: int):
+    """Run one request on the calling thread's slot: the whole circuit in one
+    registry_apply_many call, then its terminal operation."""
+    reg = d.registry_apply_many(d.registry_new(req.n, False, precision), *req.flat().arrays())
+    return _terminal(d, reg, req)
+
+
+def execute_per_gate(d, req: Request, precision: int):
+    """The plain path for one request: one gate_new + registry_apply call
+    per gate from the request's arrays, as a user of the reference module
+    writes it (doki.c:722-941)."""
+    f = req.flat()
+    reg = d.registry_new(req.n, False, precision)
+    for i in range(f.count):
+        k = int(f.op_k[i])
+        m0 = int(f.op_matrix[i])
+        g = d.gate_new(k, f.matrices[m0:m0 + (1 << (2 * k))].reshape(1 << k, 1 << k).tolist(),
+                       False)
+        cm, am = int(f.op_controls[i]), int(f.op_anticontrols[i])
+        ctl = {q for q in range(req.n) if (cm >> q) & 1} if (cm or am) else None
+        act = {q for q in range(req.n) if (am >> q) & 1} or None
+        reg = d.registry_apply(reg, g, [int(t) for t in f.op_targets[i, :k]], ctl, act, -1,
+                               False)
+    return _terminal(d, reg, req)
+
+
+def run_plain(d, reqs: Sequence[Request], precision: int = 2,
+              deadline_s: float = 3600.0) -> Dict:
+    """The plain GPU path: the requests one after another on one slot, each
+    through one registry_apply call per gate; returns its throughput and
+    the seconds each request took."""
+    t0 = time.perf_counter()
+    per = []
+    for r in reqs:
+        a = time.perf_counter()
+        execute_per_gate(d, r, precision)
+        per.append(time.perf_counter() - a)
+        if a - t0 > deadline_s:
+            raise TimeoutError(f"plain run exceeded {deadline_s} s")
+    total = time.perf_counter() - t0
+    return {"requests": len(reqs), "throughput_rps": len(reqs) / total, "seconds": per}
 
 
 class Server:

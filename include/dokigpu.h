@@ -141,6 +141,28 @@ int dk_measure(dk_state *s, unsigned target, double roll, int *result,
 int dk_measure_mask(dk_state *s, uint64_t mask, const double *rolls,
 		    unsigned num_rolls, int8_t *results, dk_state **out);
 
+/* ---- distributed registers (no counterpart in the reference) ------------
+ * The local part of a register sharded over ranks by its top qubits: each
+ * rank holds a register of the low qubits, and a gate on a rank qubit swaps
+ * that qubit with a local one by exchanging half of the local amplitudes
+ * with the partner rank.  These three calls give the rank its local view. */
+/* Once the queued gates of `s` have run: its norm constant (logical
+ * amplitude = stored amplitude / norm) and the 2-norm of its stored
+ * amplitudes (equal after a gate; a register stored as given keeps norm 1). */
+int dk_state_norm(dk_state *s, double *norm, double *stored_norm);
+/* scale x the logical amplitudes of `s` whose qubit `bit` equals `value`
+ * (2^(n-1) of them, in index order) into `dst`, in the register's storage
+ * precision (complex64 or complex128, interleaved); `dst` is device memory
+ * when on_device, else host memory (then the call waits for the copy). */
+int dk_state_read_half(dk_state *s, unsigned bit, int value, double scale, void *dst,
+		       int on_device);
+/* A new register: its amplitudes with qubit `bit` = `value` are `src`
+ * (2^(n-1), storage precision, index order; device memory when on_device),
+ * the others are scale x the logical amplitudes of `in`; stored as given
+ * (norm 1), like dk_state_from_host. */
+int dk_state_replace_half(dk_state *in, unsigned bit, int value, double scale, const void *src,
+			  int on_device, dk_state **out);
+
 /* join qops.c:97-122: tensor product, `most` on the high qubits. */
 int dk_join(dk_state *most, dk_state *least, dk_state **out);
 
@@ -211,8 +233,14 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 		   const unsigned *op_k, const unsigned *op_targets,
 		   const uint64_t *op_controls, const uint64_t *op_anticontrols,
 		   const uint64_t *op_matrix, const double *matrices, int tile_bits,
-		   dk_batch **out);
-/* CTAs per SM for the batch kernels (1..4); the autotuner's second knob. */
+		   int fold, dk_batch **out);
+/* `fold` is the dense-block fusion of the plan: a run of gates inside a
+ * 3-qubit pass becomes one 8x8 product when that costs less than applying
+ * them one by one, each gate charged its arithmetic plus `fold` FP64
+ * multiply-adds per thread of dispatch; 0 = the planner's default (96),
+ * < 0 = off (every gate applied on its own), larger values fold more
+ * readily.  The circuits are planned on all host cores.
+ * CTAs per SM for the batch kernels (1..4); the autotuner's second knob. */
 int dk_batch_set_ctas(dk_batch *b, int ctas_per_sm);
 /* Queue every circuit (captured into a CUDA graph on first use); keep_states
  * also stores each final register for dk_batch_state.  Returns before the
@@ -228,6 +256,12 @@ int dk_batch_rho_all(dk_batch *b, double *out, uint64_t *offsets);
 uint64_t dk_batch_rho_elems(const dk_batch *b);
 /* final raw amplitudes of circuit c (needs keep_states): 2 * 2^n doubles */
 int dk_batch_state(dk_batch *b, unsigned circuit, double *out);
+/* Precision form of the batch: for every circuit of two batches built from
+ * the same circuits (typically complex64 and complex128), both run with
+ * keep_states, the fidelity |<x|y>|^2 / (<x|x> <y|y>) of the final registers
+ * and the largest |x_i / |x| - y_i / |y||, computed on the device in FP64
+ * (fidelity, max_amp_err: one double per circuit). */
+int dk_batch_compare(dk_batch *x, dk_batch *y, double *fidelity, double *max_amp_err);
 const char *dk_batch_error(const dk_batch *b);
 void dk_batch_free(dk_batch *b);
 

@@ -92,3 +92,54 @@ def test_autotuner_caches(dk_gpu, small_batch, tmp_path):
     assert r1["tile_bits"] in (10, 12) and not r1["cached"]
     r2 = autotune(small_batch, 1, tile_bits=(10, 12), ctas=(1,), reps=1, cache_path=cache)
     assert r2["cached"] and r2["tile_bits"] == r1["tile_bits"]
+
+
+def test_batch_config_depths_vs_oracle(dk_gpu, orc, oracle_mod):
+    """Circuits of the batching workload itself (depth 10-50), a sample of
+    every size class, against the oracle; the fusion setting of the plan
+    changes nothing beyond rounding."""
+    from doki_b200.batch import BatchEngine
+
+    fb = W.batch_arrays(seed=4, count=4096)
+    depth = np.diff(fb.op_start.astype(np.int64)) // (fb.num_qubits + fb.num_qubits // 2)
+    idx = []
+    for n in range(4, 15):
+        cand = [int(c) for c in np.nonzero(fb.num_qubits == n)[0] if depth[c] >= 30]
+        idx += cand[:1]
+    sub = fb.subset(idx)
+    for fold in (0, -1, 400):
+        eng = BatchEngine(sub, precision=2, tile_bits=12, fold=fold)
+        eng.run(keep_states=True)
+        eng.sync()
+        rho_all, offs = eng.rho_all()
+        for c in range(sub.count):
+            psi, rho = oracle_case(orc, oracle_mod, sub, c)
+            got = eng.state(c)
+            assert np.allclose(got / np.linalg.norm(got), psi, atol=ATOL_C128, rtol=0), (fold, c)
+            dim = 1 << int(sub.keep[c])
+            r = rho_all[int(offs[c]):int(offs[c]) + dim * dim].reshape(dim, dim)
+            assert np.allclose(r, rho, atol=ATOL_C128, rtol=0), (fold, c)
+        eng.close()
+
+
+def test_batch_complex64_fidelity_against_complex128(dk_gpu, small_batch):
+    """The device comparison of a complex64 batch with the complex128 batch
+    of the same circuits equals the host computation on the exported
+    states, and the fidelity stays above 1 - 1e-6."""
+    from doki_b200.batch import BatchEngine
+
+    e64 = BatchEngine(small_batch, precision=1, tile_bits=12)
+    e128 = BatchEngine(small_batch, precision=2, tile_bits=12)
+    e64.run(keep_states=True)
+    e128.run(keep_states=True)
+    e64.sync()
+    e128.sync()
+    fid, err = e64.compare(e128)
+    assert fid.min() > 1 - 1e-6 and err.max() < 5e-5
+    for c in (0, 13, 37, small_batch.count - 1):
+        x, y = e64.state(c), e128.state(c)
+        x, y = x / np.linalg.norm(x), y / np.linalg.norm(y)
+        assert abs(fid[c] - abs(np.vdot(x, y)) ** 2) < 1e-12
+        assert abs(err[c] - np.abs(x - y).max()) < 1e-12
+    e64.close()
+    e128.close()

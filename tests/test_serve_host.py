@@ -47,6 +47,10 @@ class FakeDoki:
     def registry_apply(self, reg, g, targets, c, a, threads, verbose):
         return reg
 
+    def registry_apply_many(self, reg, *arrays):
+        assert len(arrays) == 6
+        return reg
+
     def _finish(self, reg):
         time.sleep(self.delay)
         with self.lock:
@@ -97,3 +101,14 @@ def test_request_stream_is_seeded():
         [(r.n, r.depth, r.terminal, r.mask) for r in b]
     assert all(8 <= r.n <= 28 and 10 <= r.depth <= 100 for r in a)
     assert all(r.arrival >= 0 for r in a)
+
+
+def test_plain_path_runs_one_request_at_a_time_gate_by_gate():
+    d = FakeDoki()
+    calls = []
+    d.registry_apply = lambda reg, g, t, c, a, th, v: calls.append(t) or reg
+    reqs = S.request_stream(seed=3, count=5, qmin=4, qmax=6, dmin=2, dmax=3)
+    out = S.run_plain(d, reqs, precision=2)
+    assert out["requests"] == 5 and len(out["seconds"]) == 5
+    assert d.max_live == 1
+    assert len(calls) == sum(r.flat().count for r in reqs)

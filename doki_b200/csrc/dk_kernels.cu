@@ -1102,11 +1102,14 @@ __global__ void __launch_bounds__(256, 2)
 				phase ^= 1u;
 				asm volatile("tcgen05.fence::after_thread_sync;" ::);
 				const bool ctl = (d.x & 0xffffu) == DK_GC_DENSE3 + 1;
+				/* both loads while the warp is converged (.sync.aligned),
+				 * before any per-column branch */
+				uint32_t y[2][16];
+				tm_ld16(ta + 128u + 16u * rb0, y[0]);
+				tm_ld16(ta + 128u + 16u * (rb0 + 1u), y[1]);
+				asm volatile("tcgen05.wait::ld.sync.aligned;" ::);
 #pragma unroll
 				for (int j = 0; j < 2; ++j) {
-					uint32_t y[16];
-					tm_ld16(ta + 128u + 16u * (rb0 + (uint32_t)j), y);
-					asm volatile("tcgen05.wait::ld.sync.aligned;" ::);
 					if (!ok)
 						continue;
 					if (ctl) { /* rare: controls off the pass bits */
@@ -1120,8 +1123,8 @@ __global__ void __launch_bounds__(256, 2)
 						const uint32_t so = cs[j] ^ ((r & 1) ? s0 : 0u) ^
 								    ((r & 2) ? s1 : 0u) ^ ((r & 4) ? s2 : 0u);
 						if (DK_IN_BOUNDS(so, tn_amp, CHK_SCATTER))
-							tile[so] = make_float2(__uint_as_float(y[r]),
-									       __uint_as_float(y[8 + r]));
+							tile[so] = make_float2(__uint_as_float(y[j][r]),
+									       __uint_as_float(y[j][8 + r]));
 					}
 				}
 				/* the scatters precede the next gather and the B rewrite;

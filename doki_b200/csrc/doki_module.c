@@ -24,7 +24,11 @@
  *   registry_precision(reg); registry_flush(reg); registry_compare(a, b);
  *   engine_sync();
  *   engine_set_fusion(bool); engine_stats(); engine_stream();
- *   engine_new_slot(); engine_set_slot(slot); engine_get_slot().
+ *   engine_new_slot(); engine_set_slot(slot); engine_get_slot();
+ *   registry_apply_many(reg, op_k, op_targets, op_controls, op_anticontrols,
+ *   op_matrix, matrices) -- a whole circuit in one call (serving form);
+ *   registry_norm(reg), registry_read_half(...), registry_replace_half(...)
+ *   -- the local view of a distributed register (doki_b200.dist).
  */
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>

@@ -226,7 +226,7 @@ def test_tensor_memory_sweep_wait_expires_cleanly(dk_gpu):
     read that follows reports DK_ERR_TIMEOUT (23).  The context stays
     usable: the same circuit run right after is correct."""
     r = subprocess.run([sys.executable, "-c", STARVE, LIB_DBG, ROOT],
-                       env=dict(os.environ, DK_TENSOR="1"),
+                       env=dict(os.environ, DK_TENSOR="1", DK_C64_TMEM="1"),
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-3000:])
     assert "starved 23" in r.stdout and "after 0" in r.stdout

@@ -79,6 +79,18 @@ template <int SW> __device__ __forceinline__ uint32_t swz(uint32_t i)
 	return i ^ (f & ((1u << SW) - 1u));
 }
 
+/* The tile layout of a sweep header's bank map (dk_sweep_hdr.bankv): index
+ * i sits in slot i ^ (XOR of nibble b of bankv over the set bits b of i). */
+__device__ __forceinline__ uint32_t swz_map(uint32_t i, uint64_t bankv)
+{
+	uint32_t f = 0;
+#pragma unroll
+	for (int b = 0; b < 16; ++b)
+		if ((i >> b) & 1u)
+			f ^= (uint32_t)(bankv >> (4 * b)) & 15u;
+	return i ^ f;
+}
+
 __device__ __forceinline__ bool ctl_ok(uint32_t loc, uint32_t lc, uint32_t la)
 {
 	return ((loc & lc) == lc) && !(loc & la);

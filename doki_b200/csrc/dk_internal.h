@@ -175,7 +175,14 @@ typedef struct dk_sweep_hdr {
 	uint32_t pass_off, gate_off, mat_off; /* byte offsets from the header */
 	uint32_t bytes; /* total program bytes */
 	uint32_t cond_off, ncond; /* global-condition table */
-	uint32_t pad2[2];
+	/* Shared-memory layout of the tile: tile index i sits in slot
+	 * i ^ (XOR over the set bits b of i of v_b), v_b = nibble b of bankv, a
+	 * vector over the low SW bits of the slot (SW = 3 for 16-byte, 4 for
+	 * 8-byte amplitudes; v_b = 0 for b < SW).  v_b is the bank-group
+	 * direction of tile bit b.  Scalar sweeps use v_b = 2^(b mod SW) (the
+	 * kernels' fixed XOR swizzle); tensor sweeps a map the planner picks for
+	 * the sweep's own access patterns. */
+	uint64_t bankv;
 } dk_sweep_hdr;
 
 /* Sweep execution modes.  SCALAR: the gate list holds any kinds, applied
@@ -222,6 +229,10 @@ typedef struct dk_plan_limits {
 	/* Tensor sweeps (tiles of at least 8 qubits): in 0 = on, < 0 = off;
 	 * out 1 / 0. */
 	int tensor;
+	/* Access pattern the bank map of a tensor sweep is chosen for: 0 the
+	 * mma.sync kernels' lane layout, 1 whole columns per thread (the tcgen05
+	 * complex64 kernel, 12-bit tiles). */
+	int bank_mode;
 } dk_plan_limits;
 
 void dk_plan_default_limits(int prec, unsigned n, dk_plan_limits *lim);

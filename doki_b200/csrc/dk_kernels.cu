@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 			if ((r >> j) & 1)
 				o |= 1ull << sq[lanes + j];
 		soff[r] = o;
-		sro[r] = swz<SW>((uint32_t)r << lanes);
+		sro[r] = swz_map((uint32_t)r << lanes, h->bankv);
 	}
 	for (int e = tid; e < DK_DEP_NIBBLES * 16; e += blockDim.x) {
 		uint64_t v = (uint64_t)(e & 15) << (4 * (e >> 4));
@@ -512,9 +512,10 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
 	for (int j = 0; j < lanes; ++j)
 		if ((tid >> j) & 1u)
 			off_t0 |= 1ull << sq[j];
-	const uint32_t stid0 = swz<SW>(tid);
+	const uint32_t stid0 = swz_map(tid, h->bankv);
+	const uint32_t s256 = swz_map(256u, h->bankv);
 	auto off_t = [&](int h) -> uint64_t { return h ? (off_t0 | (1ull << sq[8])) : off_t0; };
-	auto stid = [&](int h) -> uint32_t { return h ? (stid0 ^ swz<SW>(256u)) : stid0; };
+	auto stid = [&](int h) -> uint32_t { return h ? (stid0 ^ s256) : stid0; };
 	__syncthreads();
 	const uint64_t ntiles = h->ntiles;
 	const int ndep = (h->n - m + 3) >> 2;
@@ -936,7 +937,7 @@ __global__ void __launch_bounds__(256, 2)
 			if ((r >> j) & 1)
 				o |= 1ull << sq[lanes + j];
 		soff[r] = o;
-		sro[r] = swz<SW>((uint32_t)r << lanes);
+		sro[r] = swz_map((uint32_t)r << lanes, h->bankv);
 	}
 	for (int e = tid; e < DK_DEP_NIBBLES * 16; e += blockDim.x) {
 		uint64_t v = (uint64_t)(e & 15) << (4 * (e >> 4));
@@ -951,9 +952,10 @@ __global__ void __launch_bounds__(256, 2)
 	for (int j = 0; j < lanes; ++j)
 		if ((tid >> j) & 1u)
 			off_t0 |= 1ull << sq[j];
-	const uint32_t stid0 = swz<SW>(tid);
+	const uint32_t stid0 = swz_map(tid, h->bankv);
+	const uint32_t s256 = swz_map(256u, h->bankv);
 	auto off_t = [&](int hh) -> uint64_t { return hh ? (off_t0 | (1ull << sq[8])) : off_t0; };
-	auto stid = [&](int hh) -> uint32_t { return hh ? (stid0 ^ swz<SW>(256u)) : stid0; };
+	auto stid = [&](int hh) -> uint32_t { return hh ? (stid0 ^ s256) : stid0; };
 	/* passes: this thread's columns, one per row block it owns */
 	const uint32_t rb0 = 2u * (warp >> 2);
 	uint32_t col[2];

@@ -650,7 +650,214 @@ typedef struct fold_params {
 	int dispatch; /* cost of one gate on its own (0: no folding) */
 	int max_mat; /* complex matrix entries of a sweep */
 	int tensor; /* every gate list entry is an 8x8 product (tensor sweep) */
+	int bank_mode; /* dk_plan_limits.bank_mode */
 } fold_params;
+
+/* ---- bank map of a tensor sweep --------------------------------------------
+ * Under the layout of dk_sweep_hdr.bankv, tile bit b moves an access to bank
+ * group v_b (e_b for the SW low bits).  A quarter-warp of 16-byte accesses
+ * (half-warp of 8-byte ones) whose lanes vary the tile bits B takes
+ * 2^(SW - rank{v_b : b in B}) wavefronts.  The planner fixes each pass's bit
+ * orders first (with the residue model v_b = e_(b mod SW)), then picks the
+ * v_b of the bits above SW that minimise the wavefronts of the accesses the
+ * sweep's kernel makes, and derives the slot tables from the raw ones. */
+
+typedef struct bank_pat {
+	int w; /* accesses of this shape per tile */
+	int nb;
+	uint8_t b[4]; /* tile bits varied by the lanes of one wavefront group */
+} bank_pat;
+
+static int gf2_rank(const unsigned *v, int k)
+{
+	unsigned basis[4];
+	int r = 0;
+	for (int i = 0; i < k; i++) {
+		unsigned x = v[i];
+		for (int j = 0; j < r; j++)
+			if ((x ^ basis[j]) < x)
+				x ^= basis[j];
+		if (x) {
+			/* keep the basis reduced on its leading bits */
+			basis[r++] = x;
+			for (int a = r - 1; a > 0 && basis[a] > basis[a - 1]; a--) {
+				const unsigned t = basis[a];
+				basis[a] = basis[a - 1];
+				basis[a - 1] = t;
+			}
+		}
+	}
+	return r;
+}
+
+static int pat_cost(const bank_pat *p, const unsigned *F, int sw)
+{
+	unsigned v[4];
+	for (int i = 0; i < p->nb; i++)
+		v[i] = F[p->b[i]];
+	return p->w << (sw - gf2_rank(v, p->nb));
+}
+
+static int tile_bit(uint32_t mask) { return mask ? __builtin_ctz(mask) : 0; }
+
+/* The wavefront-group shapes of a tensor sweep's passes.  mode 0 (mma.sync
+ * kernels): a pass gathers with lanes on (thread bit 0 [, thread bit 1 for
+ * 8-byte amplitudes], pass bits 0, 1) and scatters with lanes on (pass bit
+ * 0 [, pass bit 1], thread bits 1, 2), twice per column group; a chained
+ * pair gathers with its first pass and scatters with its second.  mode 1
+ * (whole columns per thread): lanes on thread bits 0 .. SW-1, eight reads
+ * and eight writes per column and entry. */
+static int bank_patterns(const dk_pass_desc *pd, int npass, int sw, int mode, bank_pat *out)
+{
+	int np = 0;
+	for (int i = 0; i < npass; i++) {
+		const dk_pass_desc *a = &pd[i];
+		const int chained = mode == 0 && (a->flags & DK_PASS_CHAIN) && i + 1 < npass;
+		const dk_pass_desc *c = chained ? &pd[i + 1] : a;
+		const int nent = chained ? 1 : (a->g1 > a->g0 ? a->g1 - a->g0 : 1);
+		if (mode == 1) {
+			bank_pat *p = &out[np++];
+			p->w = 16 * nent;
+			p->nb = sw;
+			for (int j = 0; j < sw; j++)
+				p->b[j] = (uint8_t)tile_bit(a->rlo[1u << j]);
+			continue;
+		}
+		bank_pat *g = &out[np++], *t = &out[np++];
+		g->w = t->w = 2 * nent;
+		g->nb = t->nb = sw == 3 ? 3 : 4;
+		if (sw == 3) {
+			g->b[0] = (uint8_t)tile_bit(a->rlo[1]);
+			g->b[1] = (uint8_t)tile_bit(a->pm[0]);
+			g->b[2] = (uint8_t)tile_bit(a->pm[1]);
+			t->b[0] = (uint8_t)tile_bit(c->pm[0]);
+			t->b[1] = (uint8_t)tile_bit(c->rlo[2]);
+			t->b[2] = (uint8_t)tile_bit(c->rlo[4]);
+		} else {
+			g->b[0] = (uint8_t)tile_bit(a->rlo[1]);
+			g->b[1] = (uint8_t)tile_bit(a->rlo[2]);
+			g->b[2] = (uint8_t)tile_bit(a->pm[0]);
+			g->b[3] = (uint8_t)tile_bit(a->pm[1]);
+			t->b[0] = (uint8_t)tile_bit(c->pm[0]);
+			t->b[1] = (uint8_t)tile_bit(c->pm[1]);
+			t->b[2] = (uint8_t)tile_bit(c->rlo[2]);
+			t->b[3] = (uint8_t)tile_bit(c->rlo[4]);
+		}
+		if (chained)
+			i++;
+	}
+	return np;
+}
+
+/* Local search for the v_b (b >= sw) of a tile of m bits, starting from the
+ * residue map and from a few fixed pseudo-random maps; the cheapest wins
+ * (the residue map on ties).  F: m entries, F[b] = e_b for b < sw. */
+static void choose_bank_map(const bank_pat *pat, int np, int m, int sw, unsigned *F)
+{
+	const unsigned nv = 1u << sw;
+	unsigned best[16], cur[16];
+	for (int b = 0; b < m; b++)
+		best[b] = b < sw ? 1u << b : 1u << (b % sw);
+	int best_cost = 0;
+	for (int i = 0; i < np; i++)
+		best_cost += pat_cost(&pat[i], best, sw);
+	int ideal = 0;
+	for (int i = 0; i < np; i++)
+		ideal += pat[i].w;
+	uint32_t rng = 0x9e3779b9u;
+	for (int start = 0; start < 4 && best_cost > ideal; start++) {
+		for (int b = 0; b < m; b++) {
+			if (b < sw || start == 0) {
+				cur[b] = best[b];
+			} else {
+				rng = rng * 1664525u + 1013904223u;
+				cur[b] = 1u + (rng >> 8) % (nv - 1u);
+			}
+		}
+		int cost = 0;
+		for (int i = 0; i < np; i++)
+			cost += pat_cost(&pat[i], cur, sw);
+		for (int improved = 1; improved && cost > ideal;) {
+			improved = 0;
+			for (int b = sw; b < m; b++) {
+				/* cost of the patterns that use bit b, for each candidate */
+				int base = 0;
+				for (int i = 0; i < np; i++)
+					for (int j = 0; j < pat[i].nb; j++)
+						if (pat[i].b[j] == b) {
+							base += pat_cost(&pat[i], cur, sw);
+							break;
+						}
+				const unsigned keep = cur[b];
+				unsigned pick = keep;
+				int pick_cost = base;
+				for (unsigned v = 1; v < nv; v++) {
+					if (v == keep)
+						continue;
+					cur[b] = v;
+					int c = 0;
+					for (int i = 0; i < np; i++)
+						for (int j = 0; j < pat[i].nb; j++)
+							if (pat[i].b[j] == b) {
+								c += pat_cost(&pat[i], cur, sw);
+								break;
+							}
+					if (c < pick_cost) {
+						pick_cost = c;
+						pick = v;
+					}
+				}
+				cur[b] = pick;
+				if (pick != keep) {
+					cost += pick_cost - base;
+					improved = 1;
+				}
+			}
+		}
+		if (cost < best_cost) {
+			best_cost = cost;
+			memcpy(best, cur, sizeof(unsigned) * (size_t)m);
+		}
+	}
+	memcpy(F, best, sizeof(unsigned) * (size_t)m);
+}
+
+static uint32_t swizzle_map(uint32_t i, const unsigned *F, int m, int sw)
+{
+	uint32_t f = 0;
+	for (int b = sw; b < m; b++)
+		if ((i >> b) & 1u)
+			f ^= F[b];
+	return i ^ f;
+}
+
+/* Slot tables of every pass from its raw tables under the map F, and the
+ * map packed for the sweep header. */
+static uint64_t apply_bank_map(dk_pass_desc *pd, int npass, const unsigned *F, int m, int sw)
+{
+	for (int i = 0; i < npass; i++) {
+		dk_pass_desc *p = &pd[i];
+		for (int j = 0; j < DK_PASS_BITS; j++)
+			p->sp[j] = swizzle_map(p->pm[j], F, m, sw);
+		for (int x = 0; x < 32; x++)
+			p->slo[x] = swizzle_map(p->rlo[x], F, m, sw);
+		for (int y = 0; y < 16; y++)
+			p->shi[y] = swizzle_map(p->rhi[y], F, m, sw);
+	}
+	uint64_t packed = 0;
+	for (int b = sw; b < m; b++)
+		packed |= (uint64_t)(F[b] & 15u) << (4 * b);
+	return packed;
+}
+
+/* The fixed XOR swizzle of scalar sweeps as a bank map (v_b = e_(b mod sw)). */
+static uint64_t default_bank_map(int m, int sw)
+{
+	uint64_t packed = 0;
+	for (int b = sw; b < m; b++)
+		packed |= (uint64_t)(1u << (b % sw)) << (4 * b);
+	return packed;
+}
 
 /* An entry of a sweep's gate list: a source gate (op >= 0) or a folded run
  * (op < 0); m8 is the 8x8 matrix in register order for DK_GK_DENSE3. */
@@ -1158,6 +1365,23 @@ static int emit_sweep(blob_t *b, const dk_flat_op *ops, const int *idx,
 	h->bytes = (uint32_t)bytes;
 	h->cond_off = (uint32_t)cond_off;
 	h->ncond = (uint32_t)ncond;
+	if (fold->tensor && npass > 0) {
+		/* the bank map for the kernel that runs this sweep; the tcgen05
+		 * complex64 kernel (whole columns) runs 12-bit tiles only */
+		const int mode = (fold->bank_mode == 1 && prec == DK_C64 && m == 12) ? 1 : 0;
+		bank_pat *pat = (bank_pat *)malloc(sizeof(bank_pat) * 2 * (size_t)npass);
+		if (pat) {
+			unsigned F[16];
+			const int np = bank_patterns(passes, npass, res, mode, pat);
+			choose_bank_map(pat, np, m, res, F);
+			h->bankv = apply_bank_map(passes, npass, F, m, res);
+			free(pat);
+		} else {
+			h->bankv = default_bank_map(m, res);
+		}
+	} else {
+		h->bankv = default_bank_map(m, res);
+	}
 	memcpy(base + pass_off, passes, sizeof(dk_pass_desc) * (size_t)npass);
 
 	dk_gate_desc *gd = (dk_gate_desc *)(base + gate_off);
@@ -1341,7 +1565,7 @@ int dk_plan_build(const dk_flat_op *ops, int nops, unsigned n, int prec,
 	const int sweepable = (m >= DK_PASS_BITS);
 	/* tensor sweeps need a full warp of 8-amplitude columns per tile */
 	const fold_params fold = { lim->fold > 0 ? lim->fold : 0, lim->max_mat,
-				   lim->tensor > 0 && m >= DK_PASS_BITS + 5 };
+				   lim->tensor > 0 && m >= DK_PASS_BITS + 5, lim->bank_mode };
 	for (int i = 0; i < nops; i++) {
 		rem[i] = i;
 		kinds[i] = (ops[i].k <= DK_SWEEP_MAX_K && sweepable)

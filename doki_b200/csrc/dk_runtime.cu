@@ -273,6 +273,9 @@ int flush(dk_state *s)
 	lim.tensor = g.tensor;
 	dk_plan_default_limits(prec, n, &lim);
 	lim.fuse = g.fuse;
+	/* complex64 tensor sweeps of 12-bit tiles run on the tcgen05 kernel
+	 * (whole columns per thread) unless DK_C64_TMEM=0 */
+	lim.bank_mode = (prec == DK_C64 && dk::g_c64_tmem) ? 1 : 0;
 	if (g.low_bits >= 0 && g.low_bits <= lim.tile_bits)
 		lim.low_bits = g.low_bits;
 	dk_plan plan;

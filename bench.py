@@ -51,7 +51,14 @@ def parse():
                    help="one sweep per gate (the per-gate plain method)")
     p.add_argument("--no-forms", action="store_true",
                    help="skip the batching / serving / precision forms")
-    p.add_argument("--serve-requests", type=int, default=120)
+    p.add_argument("--serve-requests", type=int, default=400,
+                   help="requests of the seeded 20,000-request stream the serving form "
+                        "runs (a prefix of it)")
+    p.add_argument("--serve-plain", type=int, default=600,
+                   help="requests the plain path runs (a prefix); its throughput on the "
+                        "served sample is scaled from their times by qubit count")
+    p.add_argument("--serve-only", action="store_true",
+                   help="run only the serving form and print its JSON object")
     p.add_argument("--precision", choices=("c128", "c64"), default="c128",
                    help="register precision of the plain workload (c64: split-TF32 "
                         "tensor products, FP64 norms)")
@@ -466,7 +473,21 @@ def batch_form(d, torch):
     return res
 
 
-def serve_form(d, count):
+def plain_rate(per_n_seconds, hist):
+    """Throughput of the one-at-a-time plain path on a request mix with qubit
+    histogram `hist`, from measured seconds per request grouped by qubit
+    count (additive: requests run one after another)."""
+    total = 0.0
+    for n, cnt in hist.items():
+        times = per_n_seconds.get(n)
+        if not times:  # no sample of this size: its nearest measured size
+            near = min(per_n_seconds, key=lambda m: abs(m - n))
+            times = per_n_seconds[near]
+        total += cnt * statistics.mean(times)
+    return sum(hist.values()) / total
+
+
+def serve_form(d, count, plain_count=600):
     import numpy as np
     from doki_b200 import serve as S
     stream = S.request_stream(seed=5, count=20000)
@@ -475,7 +496,7 @@ def serve_form(d, count):
     sample = (f"the first {count} requests of the seeded 20,000-request stream "
               "(n log-uniform [8,28], depth U[10,100], probabilities or 1-8 measurements); "
               "circuits prepared as data before the runs")
-    srv = S.Server(d, workers=8, budget_bytes=150e9, precision=1, deadline_s=900)
+    srv = S.Server(d, workers=8, budget_bytes=150e9, precision=1, deadline_s=3600)
     cap = srv.run(S.with_rate(reqs, 1e9))
     out = {"sample": sample, "workers": 8, "budget_bytes": 150e9, "precision": "c64",
            "submission": "one registry_apply_many call per request",
@@ -484,16 +505,27 @@ def serve_form(d, count):
         r = srv.run(S.with_rate(reqs, load * cap["throughput_rps"]))
         out["loads"][f"{int(load * 100)}%"] = {k: r[k] for k in
                                               ("throughput_rps", "p50_ms", "p99_ms")}
+    ns = np.array([r.n for r in reqs])
+    hist = {int(n): int((ns == n).sum()) for n in np.unique(ns)}
+    pc = min(plain_count, count)
     plain = {}
     for prec, name in ((2, "c128"), (1, "c64")):
-        p = S.run_plain(d, reqs, precision=prec, deadline_s=1800)
-        plain[name] = p["throughput_rps"]
+        p = S.run_plain(d, reqs[:pc], precision=prec, deadline_s=3600)
+        per_n = {}
+        for r, t in zip(reqs[:pc], p["seconds"]):
+            per_n.setdefault(r.n, []).append(t)
+        plain[name] = {"measured_rps": p["throughput_rps"],
+                       "rps": p["throughput_rps"] if pc == count else plain_rate(per_n, hist)}
     out["plain"] = {"path": "one request at a time, one registry_apply call per gate",
-                    "c128_rps": plain["c128"], "c64_rps": plain["c64"]}
-    out["speedup_vs_plain_c128"] = cap["throughput_rps"] / plain["c128"]
-    out["speedup_vs_plain_c64"] = cap["throughput_rps"] / plain["c64"]
-    ns = np.array([r.n for r in reqs])
-    out["qubits_histogram"] = {int(n): int((ns == n).sum()) for n in np.unique(ns)}
+                    "measured_on": f"the first {pc} requests"
+                                   + ("" if pc == count else
+                                      f", scaled to the {count}-request sample by qubit count"),
+                    "c128_rps": plain["c128"]["rps"], "c64_rps": plain["c64"]["rps"],
+                    "c128_measured_rps": plain["c128"]["measured_rps"],
+                    "c64_measured_rps": plain["c64"]["measured_rps"]}
+    out["speedup_vs_plain_c128"] = cap["throughput_rps"] / plain["c128"]["rps"]
+    out["speedup_vs_plain_c64"] = cap["throughput_rps"] / plain["c64"]["rps"]
+    out["qubits_histogram"] = hist
     return out
 
 
@@ -514,7 +546,7 @@ def precision_form(d):
 def run_forms(d, args, torch):
     forms = {}
     for name, fn in (("batch", lambda: batch_form(d, torch)),
-                     ("serve", lambda: serve_form(d, args.serve_requests)),
+                     ("serve", lambda: serve_form(d, args.serve_requests, args.serve_plain)),
                      ("precision", lambda: precision_form(d))):
         try:
             forms[name] = fn()
@@ -687,11 +719,24 @@ def reference_arm(args, rank, world):
     }), flush=True)
 
 
+def serve_only(args):
+    """The serving form alone (for runs over the whole request stream)."""
+    import doki_b200
+    d = doki_b200.load()
+    t0 = time.perf_counter()
+    out = serve_form(d, args.serve_requests, args.serve_plain)
+    out["wall_s"] = time.perf_counter() - t0
+    print(json.dumps({"form": "serve", **out}), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.serve_only:
+        serve_only(args)
+        return
     if args.impl == "reference":
         reference_arm(args, rank, world)
     else:

@@ -36,3 +36,12 @@ def test_cpu_baseline_measures_a_whole_layer():
     assert cb["layer"]["gates"] == len(bench.layer_ops(c))
     assert cb["value"] > 0 and cb["one_thread"]["cores"] == 1
     assert "measured whole" in cb["sample"]
+
+
+def test_plain_rate_scales_by_qubit_count():
+    """One-at-a-time throughput from per-size means: 3 requests of 10 qubits
+    at 1 s and 1 of 20 qubits at 5 s take 8 s for 4 requests."""
+    per_n = {10: [0.5, 1.5], 20: [5.0]}
+    assert abs(bench.plain_rate(per_n, {10: 3, 20: 1}) - 4 / 8.0) < 1e-12
+    # a size without a sample borrows the nearest measured size
+    assert abs(bench.plain_rate(per_n, {11: 2}) - 2 / 2.0) < 1e-12

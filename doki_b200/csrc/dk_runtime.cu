@@ -270,7 +270,10 @@ int flush(dk_state *s)
 	dk_plan_limits lim = {};
 	lim.tile_bits = g.tile_bits;
 	lim.fold = g.fold;
-	lim.tensor = g.tensor;
+	/* one gate per sweep: nothing to fold into tensor-core products, and
+	 * each sweep is a pure stream of the register, best on the scalar
+	 * kernel with its 4 pinned low qubits (256-byte runs) */
+	lim.tensor = g.fuse ? g.tensor : -1;
 	dk_plan_default_limits(prec, n, &lim);
 	lim.fuse = g.fuse;
 	/* complex64 tensor sweeps of 12-bit tiles run on the tcgen05 kernel

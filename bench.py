@@ -225,7 +225,8 @@ def per_gate_record(d, c, prec, torch, stream, layers=2):
     and anticontrols (amplitudes whose conditions fail need not move);
     achieved = their sum / the sweeps' device time."""
     n = c.num_qubits
-    ops = c.ops[:c.layer_starts[layers]]
+    layers = min(layers, c.depth)
+    ops = c.ops[:c.layer_starts[layers]] if layers < c.depth else c.ops
     state_bytes = (8 if prec == "c64" else 16) << n
     gates = [d.gate_new(op.k, op.gate.tolist(), False) for op in ops]
     reg = d.registry_new(n, False) if prec == "c128" else d.registry_new(n, False, 1)

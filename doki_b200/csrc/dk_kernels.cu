@@ -892,12 +892,20 @@ __global__ void __launch_bounds__(256, 2)
 	const uint32_t tn_amp = 1u << M;
 	const int ncond = (int)h->ncond;
 	const size_t gate_bytes = (size_t)ngate * sizeof(dk_gate_desc);
-	C2 *const tile = reinterpret_cast<C2 *>(sm);
-	uint4 *sg = reinterpret_cast<uint4 *>(sm + sizeof(C2) * tn_amp);
+	const size_t cond_bytes = (size_t)ncond * sizeof(dk_gate_cond);
+	const int nmat = (int)((h->bytes - h->mat_off) / 16); /* complex entries */
+	/* dynamic shared memory: two tile buffers (the next tile streams in
+	 * while this one is processed), the gate list and conditions, the pass
+	 * descriptors and the matrices in float2 (read per pass and entry
+	 * without a global-memory round trip) */
+	C2 *const bufs = reinterpret_cast<C2 *>(sm);
+	uint4 *sg = reinterpret_cast<uint4 *>(sm + 2 * sizeof(C2) * tn_amp);
 	dk_gate_cond *scond =
 		reinterpret_cast<dk_gate_cond *>(reinterpret_cast<unsigned char *>(sg) + gate_bytes);
-	const dk_pass_desc *passes = reinterpret_cast<const dk_pass_desc *>(prog + h->pass_off);
-	const double2 *mats = reinterpret_cast<const double2 *>(prog + h->mat_off);
+	dk_pass_desc *passes = reinterpret_cast<dk_pass_desc *>(
+		reinterpret_cast<unsigned char *>(scond) + cond_bytes);
+	float2 *mats = reinterpret_cast<float2 *>(reinterpret_cast<unsigned char *>(passes) +
+						  (size_t)npass * sizeof(dk_pass_desc));
 	__shared__ __align__(1024) float sB[2][256]; /* R^T hi, lo */
 	__shared__ __align__(8) uint64_t mbar;
 	__shared__ uint32_t tslot;
@@ -914,6 +922,16 @@ __global__ void __launch_bounds__(256, 2)
 		uint4 *cdst = reinterpret_cast<uint4 *>(scond);
 		for (int i = tid; i < ncond; i += blockDim.x)
 			cdst[i] = __ldg(csrc + i);
+		const uint4 *psrc = reinterpret_cast<const uint4 *>(prog + h->pass_off);
+		uint4 *pdst = reinterpret_cast<uint4 *>(passes);
+		const int pwords = npass * (int)(sizeof(dk_pass_desc) / 16);
+		for (int i = tid; i < pwords; i += blockDim.x)
+			pdst[i] = __ldg(psrc + i);
+		const double2 *msrc = reinterpret_cast<const double2 *>(prog + h->mat_off);
+		for (int i = tid; i < nmat; i += blockDim.x) {
+			const double2 v = __ldg(msrc + i);
+			mats[i] = make_float2((float)v.x, (float)v.y);
+		}
 		for (int i = tid; i < 16; i += blockDim.x)
 			sq[i] = h->qpos[i];
 	}
@@ -994,7 +1012,7 @@ __global__ void __launch_bounds__(256, 2)
 		return ntiles;
 	};
 	[[maybe_unused]] const uint64_t nglob = 1ull << h->n;
-	auto prefetch = [&](uint64_t base) {
+	auto prefetch = [&](uint64_t base, C2 *tile) {
 #pragma unroll
 		for (int hh = 0; hh < 2; ++hh) {
 			const uint64_t bo = base | off_t(hh);
@@ -1016,12 +1034,18 @@ __global__ void __launch_bounds__(256, 2)
 	bool fault = false;
 	uint64_t t = next_tile(blockIdx.x);
 	if (t < ntiles)
-		prefetch(tile_base(t));
+		prefetch(tile_base(t), bufs);
+	int cur = 0;
 	while (t < ntiles && !fault) {
 		const uint64_t base = tile_base(t);
-		uint64_t tn = ntiles;
+		C2 *const tile = bufs + (size_t)cur * tn_amp;
 		cp_async_wait_all();
 		__syncthreads();
+		/* the next tile streams into the other buffer (read out, and the
+		 * barrier above passed, one tile ago) while this one is processed */
+		const uint64_t tn = next_tile(t + gridDim.x);
+		if (tn < ntiles)
+			prefetch(tile_base(tn), bufs + (size_t)(cur ^ 1) * tn_amp);
 		if (skip_idle) {
 #pragma unroll
 			for (int hh = 0; hh < 2; ++hh)
@@ -1035,14 +1059,13 @@ __global__ void __launch_bounds__(256, 2)
 		}
 		for (int p = 0; p < npass && !fault; ++p) {
 			const dk_pass_desc *pd = passes + p;
-			const uint32_t s0 = __ldg(&pd->sp[0]), s1 = __ldg(&pd->sp[1]),
-				       s2 = __ldg(&pd->sp[2]);
+			const uint32_t s0 = pd->sp[0], s1 = pd->sp[1], s2 = pd->sp[2];
 			uint32_t cs[2];
 #pragma unroll
 			for (int j = 0; j < 2; ++j)
-				cs[j] = __ldg(&pd->slo[col[j] & 31u]) ^ __ldg(&pd->shi[col[j] >> 5]);
-			const int g1 = __ldg(&pd->g1);
-			for (int g = __ldg(&pd->g0); g < g1; ++g) {
+				cs[j] = pd->slo[col[j] & 31u] ^ pd->shi[col[j] >> 5];
+			const int g1 = pd->g1;
+			for (int g = pd->g0; g < g1; ++g) {
 				const uint4 d = sg[g];
 				const uint32_t gi = d.y & 0xffffu;
 				if (gi != 0xffffu) {
@@ -1050,12 +1073,11 @@ __global__ void __launch_bounds__(256, 2)
 					if (((base & c.gc) != c.gc) || (base & c.ga))
 						continue; /* the same for every thread */
 				}
-				const double2 *mt = mats + 64 * (size_t)tc_matrix(d, scond, base);
+				const float2 *mt = mats + 64 * (size_t)tc_matrix(d, scond, base);
 				{ /* B = R, entry (n, k), split into hi and lo */
 					const int n = (int)(tid >> 4), k = (int)(tid & 15u);
-					const double2 e = __ldg(mt + 8 * (n & 7) + (k & 7));
-					const float v = ((n < 8) == (k < 8)) ? (float)e.x
-						       : (n < 8 ? -(float)e.y : (float)e.y);
+					const float2 e = mt[8 * (n & 7) + (k & 7)];
+					const float v = ((n < 8) == (k < 8)) ? e.x : (n < 8 ? -e.y : e.y);
 					uint32_t hi, lo;
 					tf32_split(v, hi, lo);
 					const int o = umma_b_off(n, k);
@@ -1115,8 +1137,7 @@ __global__ void __launch_bounds__(256, 2)
 					if (!ok)
 						continue;
 					if (ctl) { /* rare: controls off the pass bits */
-						const uint32_t raw = __ldg(&pd->rlo[col[j] & 31u]) |
-								     __ldg(&pd->rhi[col[j] >> 5]);
+						const uint32_t raw = pd->rlo[col[j] & 31u] | pd->rhi[col[j] >> 5];
 						if (!ctl_ok(raw, d.z, d.w))
 							continue;
 					}
@@ -1152,11 +1173,8 @@ __global__ void __launch_bounds__(256, 2)
 					__stcs(out + (bo | soff[r]), v);
 			}
 		}
-		__syncthreads(); /* the buffer is free */
-		tn = next_tile(t + gridDim.x);
-		if (tn < ntiles)
-			prefetch(tile_base(tn));
 		t = tn;
+		cur ^= 1;
 	}
 	cp_async_wait_all();
 	if (fault) {
@@ -2144,6 +2162,20 @@ std::atomic<int> g_tm_ran{0};
 
 /* ---------------------------------------------------------------------- */
 
+/* Persistent sweeps walk tiles t = block, block + grid, ...  An in-place
+ * sweep skips the tiles where its gates' conditions on qubits outside the
+ * tile fail; such a condition is one bit of the tile number, so with an
+ * even grid every block would see that bit fixed and half the blocks would
+ * own all the work.  An odd grid makes each block's stride visit both
+ * values of every tile-number bit. */
+static uint64_t skip_balanced_grid(uint64_t blocks, const void *in, const void *out,
+				   const dk_sweep_hdr *hp)
+{
+	if (in == out && !hp->all_touched && blocks > 1 && !(blocks & 1u))
+		blocks--;
+	return blocks;
+}
+
 template <typename R, int SW, int M, int MINB, int NBUF>
 static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dprog,
 			     const dk_sweep_hdr *hp, int num_sms, const Scratch &s,
@@ -2181,6 +2213,7 @@ static cudaError_t run_sweep(const void *in, void *out, const unsigned char *dpr
 	const uint64_t cap = (uint64_t)num_sms * MINB;
 	if (blocks > cap)
 		blocks = cap;
+	blocks = skip_balanced_grid(blocks, in, out, hp);
 	kern<<<(int)blocks, 1 << (m - DK_PASS_BITS), smem, st>>>((const C2 *)in, (C2 *)out,
 								   dprog, s.partials);
 	*blocks_out = (int)blocks;
@@ -2220,6 +2253,7 @@ static cudaError_t run_sweep_tc(const void *in, void *out, const unsigned char *
 	const uint64_t cap = (uint64_t)num_sms * MINB;
 	if (blocks > cap)
 		blocks = cap;
+	blocks = skip_balanced_grid(blocks, in, out, hp);
 	kern<<<(int)blocks, m >= 12 ? 256 : 1 << (m - DK_PASS_BITS), smem, st>>>((const C2 *)in, (C2 *)out,
 								   dprog, s.partials);
 	*blocks_out = (int)blocks;
@@ -2230,13 +2264,19 @@ static cudaError_t run_sweep_tc(const void *in, void *out, const unsigned char *
  * SM holds more than two CTAs of it (or of any kernel with the same floor)
  * and their 2 x 256 tensor-memory columns always fit in the SM's 512. */
 constexpr size_t kTmSmemFloor = 80u << 10;
+/* and at most this much, so that two of them fit on an SM */
+constexpr size_t kTmSmemMax = 104u << 10;
 
 static cudaError_t run_sweep_tm(const void *in, void *out, const unsigned char *dprog,
 				const dk_sweep_hdr *hp, int num_sms, const Scratch &s,
 				cudaStream_t st, int *blocks_out)
 {
-	size_t smem = (sizeof(float2) << 12) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
-		      (size_t)hp->ncond * sizeof(dk_gate_cond);
+	size_t smem = 2 * (sizeof(float2) << 12) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
+		      (size_t)hp->ncond * sizeof(dk_gate_cond) +
+		      (size_t)hp->npass * sizeof(dk_pass_desc) +
+		      sizeof(float2) * ((hp->bytes - hp->mat_off) / 16);
+	if (smem > kTmSmemMax)
+		return cudaErrorNotSupported; /* the caller runs the sweep on mma.sync */
 	if (smem < kTmSmemFloor)
 		smem = kTmSmemFloor;
 	auto kern = k_sweep_tm<4>;
@@ -2263,6 +2303,7 @@ static cudaError_t run_sweep_tm(const void *in, void *out, const unsigned char *
 	const uint64_t cap = (uint64_t)num_sms * 2;
 	if (blocks > cap)
 		blocks = cap;
+	blocks = skip_balanced_grid(blocks, in, out, hp);
 	kern<<<(int)blocks, 256, smem, st>>>((const float2 *)in, (float2 *)out, dprog,
 					     s.partials);
 	*blocks_out = (int)blocks;
@@ -2301,8 +2342,12 @@ cudaError_t launch_sweep(int prec, const void *in, void *out,
 	int blocks = 0;
 	cudaError_t e;
 	if (hp->mode == DK_SWEEP_TENSOR && prec == DK_C64 && m == 12 && g_c64_tmem) {
-		/* complex64, 12-bit tiles: tcgen05 TF32 products in tensor memory */
+		/* complex64, 12-bit tiles: tcgen05 TF32 products in tensor memory
+		 * (a sweep whose tables exceed the kernel's shared memory runs on
+		 * the mma.sync kernel below) */
 		e = run_sweep_tm(in, out, dprog, hp, num_sms, s, st, &blocks);
+		if (e == cudaErrorNotSupported)
+			goto mma_sync;
 		if (e != cudaSuccess)
 			return e;
 		const int all = hp->all_touched || (in != out);
@@ -2310,6 +2355,7 @@ cudaError_t launch_sweep(int prec, const void *in, void *out,
 		g_launches += 2;
 		return cudaGetLastError();
 	}
+mma_sync:
 	if (hp->mode == DK_SWEEP_TENSOR) {
 		/* tensor-core passes (FP64 for complex128, split TF32 for
 		 * complex64); tiles of 8 to 12 bits */

@@ -516,14 +516,18 @@ def serve_form(d, count, plain_count=600):
         for r, t in zip(reqs[:pc], p["seconds"]):
             per_n.setdefault(r.n, []).append(t)
         plain[name] = {"measured_rps": p["throughput_rps"],
-                       "rps": p["throughput_rps"] if pc == count else plain_rate(per_n, hist)}
+                       "rps": p["throughput_rps"] if pc == count else plain_rate(per_n, hist),
+                       "mean_ms_by_qubits": {int(k): round(1e3 * statistics.mean(v), 3)
+                                             for k, v in sorted(per_n.items())}}
     out["plain"] = {"path": "one request at a time, one registry_apply call per gate",
                     "measured_on": f"the first {pc} requests"
                                    + ("" if pc == count else
                                       f", scaled to the {count}-request sample by qubit count"),
                     "c128_rps": plain["c128"]["rps"], "c64_rps": plain["c64"]["rps"],
                     "c128_measured_rps": plain["c128"]["measured_rps"],
-                    "c64_measured_rps": plain["c64"]["measured_rps"]}
+                    "c64_measured_rps": plain["c64"]["measured_rps"],
+                    "c128_mean_ms_by_qubits": plain["c128"]["mean_ms_by_qubits"],
+                    "c64_mean_ms_by_qubits": plain["c64"]["mean_ms_by_qubits"]}
     out["speedup_vs_plain_c128"] = cap["throughput_rps"] / plain["c128"]["rps"]
     out["speedup_vs_plain_c64"] = cap["throughput_rps"] / plain["c64"]["rps"]
     out["qubits_histogram"] = hist

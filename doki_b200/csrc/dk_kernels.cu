@@ -424,19 +424,15 @@ template <> struct TcFrag<float> {
 		tf32_split(x1.x, r1h, r1l);
 		tf32_split(x0.y, i0h, i0l);
 		tf32_split(x1.y, i1h, i1l);
-		/* the two k-steps accumulate separately (two dependency chains),
-		 * small terms first */
-		float u[4] = { 0.0f, 0.0f, 0.0f, 0.0f };
+		/* one accumulation chain over both k-steps, small terms first
+		 * (no final add of two partial sums) */
 		y[0] = y[1] = y[2] = y[3] = 0.0f;
 		mma_tf32(y, k0l, r0h, r1h);
-		mma_tf32(u, k1l, i0h, i1h);
+		mma_tf32(y, k1l, i0h, i1h);
 		mma_tf32(y, k0h, r0l, r1l);
-		mma_tf32(u, k1h, i0l, i1l);
+		mma_tf32(y, k1h, i0l, i1l);
 		mma_tf32(y, k0h, r0h, r1h);
-		mma_tf32(u, k1h, i0h, i1h);
-#pragma unroll
-		for (int i = 0; i < 4; ++i)
-			y[i] += u[i];
+		mma_tf32(y, k1h, i0h, i1h);
 	}
 };
 
@@ -767,30 +763,36 @@ __global__ void __launch_bounds__(1 << ((M < 11 ? M : 11) - DK_PASS_BITS), MINB)
  * the pass bits) are the rows of A; one entry is
  *     Y^T (512 x 16) = X^T (512 x 16) R^T,   R = [[Mr, -Mi], [Mi, Mr]],
  * x = (re0..re7, im0..im7) of a column, as 4 row blocks of M = 128 (one
- * tensor-memory lane per column), N = 16, K = 16 (two k-steps of 8).
- * Operands are split into TF32 hi + lo parts (as in the mma.sync form) and
- * each block takes lo*hi + hi*lo + hi*hi, accumulated in FP32 in tensor
- * memory.  A lives in tensor memory (written by the threads that gathered
- * the columns, tcgen05.st), B (R^T hi / lo, 1 KiB each) in shared memory in
- * the K-major layout without swizzle, D in tensor memory; one thread issues
- * the 24 MMAs and commits them to an mbarrier, and every thread reads back
- * its own rows (tcgen05.ld), so a column never leaves the thread that owns
- * it between gather and scatter.
+ * tensor-memory lane per column), K = 16 (two k-steps of 8).  Operands are
+ * split into TF32 hi + lo parts (as in the mma.sync form).  B of an entry is
+ * B' = [R_hi; R_lo] (32 x 16), so one N = 32 product A_hi B'^T gives
+ * hi*hi in D columns 0..15 and hi*lo in 16..31, and an N = 16 product
+ * A_lo R_hi^T accumulates lo*hi into 16..31: four MMAs per row block, and
+ * y = D[0..15] + D[16..31] (the small terms summed apart from hi*hi).  A
+ * lives in tensor memory (written by the threads that gathered the columns,
+ * tcgen05.st), B' in shared memory in the K-major layout without swizzle
+ * (split once per CTA for all matrices of the sweep when they fit, else per
+ * entry), D in tensor memory.  The two warpgroups work on separate halves
+ * of the tile: each gathers its two row blocks, passes a 128-thread barrier,
+ * has one thread issue its 8 MMAs and commit them to its own mbarrier, and
+ * reads back its own rows (tcgen05.ld), so a column never leaves the thread
+ * that owns it between gather and scatter, and one half's MMAs run while the
+ * other half gathers or scatters.
  *
- * Tensor-memory columns per CTA (256): A hi [0, 64), A lo [64, 128),
- * D [128, 192) -- 16 per row block.  The launch keeps at most two CTAs of
- * any such kernel per SM (shared memory), so 2 x 256 <= 512 columns and the
- * allocation never waits.  Warp w owns row blocks 2 (w / 4) and
- * 2 (w / 4) + 1 in lanes 32 (w % 4) .. + 31: column c = 128 b + 32 (w % 4) +
- * lane.  Every wait on the MMAs is bounded: on expiry the kernel counts the
- * fault in g_dk_tm_fault, waits (bounded) for the MMAs in flight, frees its
- * tensor memory and returns; the host reports DK_ERR_TIMEOUT at the next
- * read. */
+ * Tensor-memory columns per CTA (256): A hi [0, 64), A lo [64, 128) -- 16
+ * per row block -- and D [128, 256), 32 per row block.  The launch keeps at
+ * most two CTAs of any such kernel per SM (shared memory), so 2 x 256 <= 512
+ * columns and the allocation never waits.  Warp w owns row blocks 2 (w / 4)
+ * and 2 (w / 4) + 1 in lanes 32 (w % 4) .. + 31: column c = 128 b +
+ * 32 (w % 4) + lane.  Every wait on the MMAs is bounded: on expiry the
+ * kernel counts the fault in g_dk_tm_fault, waits (bounded) for the MMAs in
+ * flight, frees its tensor memory and returns; the host reports
+ * DK_ERR_TIMEOUT at the next read. */
 __device__ unsigned int g_dk_tm_fault;
 #ifdef DK_DEBUG_CHECKS
-/* Debug builds only, a test hook: while set, the issuing thread of a tcgen05
- * sweep issues no MMA and no commit, so every wait runs out on an mbarrier
- * that nothing arrives at (dk_debug_tm_starve). */
+/* Debug builds only, a test hook: while set, the issuing threads of a
+ * tcgen05 sweep issue no MMA and no commit, so every wait runs out on an
+ * mbarrier that nothing arrives at (dk_debug_tm_starve). */
 __device__ int g_dk_tm_starve;
 #define DK_TM_STARVED() (g_dk_tm_starve != 0)
 #else
@@ -802,6 +804,8 @@ constexpr int kTmCols = 256; /* tensor-memory columns per CTA */
  * poll count is a second bound in case the timer does not advance. */
 constexpr unsigned long long kTmWaitNs = 1000000000ull;
 constexpr int kTmWaitPolls = 1 << 26;
+/* floats of one B' operand: two k-steps of 32 rows x 8 */
+constexpr int kTmBFloats = 512;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -817,23 +821,27 @@ __device__ __forceinline__ uint64_t umma_desc_k(uint32_t addr)
 	       ((uint64_t)(256u >> 4) << 32) | ((uint64_t)1 << 46);
 }
 
-/* Offset (in floats) of R(n, k) in a B buffer of that layout: k-steps of 8
- * at 128 floats (512 B), 8-row groups at 64, K chunks of 4 at 32, rows at 4. */
+/* Offset (in floats) of B'(n, k), n < 32, in a buffer of that layout:
+ * k-steps of 8 at 256 floats (1 KiB), 8-row groups at 64, K chunks of 4 at
+ * 32, rows at 4. */
 __device__ __forceinline__ int umma_b_off(int n, int k)
 {
-	return (k >> 3) * 128 + (n >> 3) * 64 + ((k & 7) >> 2) * 32 + (n & 7) * 4 + (k & 3);
+	return (k >> 3) * 256 + (n >> 3) * 64 + ((k & 7) >> 2) * 32 + (n & 7) * 4 + (k & 3);
 }
 
-/* kind::tf32, D f32, A and B K-major, M = 128, N = 16 */
-constexpr uint32_t kTmIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((16u >> 3) << 17) |
-			      ((128u >> 4) << 24);
+/* kind::tf32, D f32, A and B K-major, M = 128, N = 16 or 32 */
+constexpr uint32_t kTmIdesc16 = (1u << 4) | (2u << 7) | (2u << 10) | ((16u >> 3) << 17) |
+				((128u >> 4) << 24);
+constexpr uint32_t kTmIdesc32 = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) |
+				((128u >> 4) << 24);
 
-__device__ __forceinline__ void umma_tf32_ts(uint32_t d, uint32_t a, uint64_t b, uint32_t acc)
+__device__ __forceinline__ void umma_tf32_ts(uint32_t d, uint32_t a, uint64_t b, uint32_t idesc,
+					     uint32_t acc)
 {
 	const uint32_t zero = 0;
 	asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
 		     "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n\t}"
-		     ::"r"(d), "r"(a), "l"(b), "r"(kTmIdesc), "r"(acc), "r"(zero));
+		     ::"r"(d), "r"(a), "l"(b), "r"(idesc), "r"(acc), "r"(zero));
 }
 
 __device__ __forceinline__ void tm_st16(uint32_t ta, const uint32_t (&v)[16])
@@ -876,10 +884,29 @@ __device__ __forceinline__ bool tm_wait(uint32_t mbar, uint32_t parity)
 	return false;
 }
 
+/* Write B' = [R_hi; R_lo] of one 8x8 complex matrix (64 complex entries in
+ * register order, entry (r, c) at 8 r + c) into `b` (kTmBFloats floats),
+ * element e of the 256 of R handled by the calling thread for e = e0,
+ * e0 + stride, ... */
+template <typename E>
+__device__ __forceinline__ void tm_write_b(float *b, const E *mt, int e0, int stride)
+{
+	for (int e = e0; e < 256; e += stride) {
+		const int n = e >> 4, k = e & 15;
+		const E x = mt[8 * (n & 7) + (k & 7)];
+		const float re = (float)x.x, im = (float)x.y;
+		const float v = ((n < 8) == (k < 8)) ? re : (n < 8 ? -im : im);
+		uint32_t hi, lo;
+		tf32_split(v, hi, lo);
+		b[umma_b_off(n, k)] = __uint_as_float(hi);
+		b[umma_b_off(n + 16, k)] = __uint_as_float(lo);
+	}
+}
+
 template <int SW>
 __global__ void __launch_bounds__(256, 2)
 	k_sweep_tm(const float2 *__restrict__ in, float2 *out, const unsigned char *__restrict__ prog,
-		   double *partials)
+		   double *partials, int pre)
 {
 	typedef float2 C2;
 	constexpr int M = 12;
@@ -888,6 +915,7 @@ __global__ void __launch_bounds__(256, 2)
 	const int m = h->m; /* == 12 (checked by the launcher) */
 	const int lanes = m - PB;
 	const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+	const uint32_t wg = warp >> 2; /* warpgroup: row blocks 2 wg, 2 wg + 1 */
 	const int npass = h->npass, ngate = h->ngate;
 	const uint32_t tn_amp = 1u << M;
 	const int ncond = (int)h->ncond;
@@ -896,18 +924,21 @@ __global__ void __launch_bounds__(256, 2)
 	const int nmat = (int)((h->bytes - h->mat_off) / 16); /* complex entries */
 	/* dynamic shared memory: two tile buffers (the next tile streams in
 	 * while this one is processed), the gate list and conditions, the pass
-	 * descriptors and the matrices in float2 (read per pass and entry
-	 * without a global-memory round trip) */
+	 * descriptors, and at a 1 KiB offset the matrices: every B' of the
+	 * sweep (pre != 0) or the matrices in float2 for a per-entry B' */
 	C2 *const bufs = reinterpret_cast<C2 *>(sm);
 	uint4 *sg = reinterpret_cast<uint4 *>(sm + 2 * sizeof(C2) * tn_amp);
 	dk_gate_cond *scond =
 		reinterpret_cast<dk_gate_cond *>(reinterpret_cast<unsigned char *>(sg) + gate_bytes);
 	dk_pass_desc *passes = reinterpret_cast<dk_pass_desc *>(
 		reinterpret_cast<unsigned char *>(scond) + cond_bytes);
-	float2 *mats = reinterpret_cast<float2 *>(reinterpret_cast<unsigned char *>(passes) +
-						  (size_t)npass * sizeof(dk_pass_desc));
-	__shared__ __align__(1024) float sB[2][256]; /* R^T hi, lo */
-	__shared__ __align__(8) uint64_t mbar;
+	const size_t mats_at =
+		(2 * sizeof(C2) * tn_amp + gate_bytes + cond_bytes +
+		 (size_t)npass * sizeof(dk_pass_desc) + 1023) & ~(size_t)1023;
+	float *const mats_b = reinterpret_cast<float *>(sm + mats_at);
+	float2 *const mats = reinterpret_cast<float2 *>(sm + mats_at);
+	__shared__ __align__(1024) float sB[kTmBFloats]; /* per-entry B' */
+	__shared__ __align__(8) uint64_t mbar[2];
 	__shared__ uint32_t tslot;
 	__shared__ uint8_t sq[16];
 	__shared__ uint64_t soff[NA];
@@ -928,15 +959,24 @@ __global__ void __launch_bounds__(256, 2)
 		for (int i = tid; i < pwords; i += blockDim.x)
 			pdst[i] = __ldg(psrc + i);
 		const double2 *msrc = reinterpret_cast<const double2 *>(prog + h->mat_off);
-		for (int i = tid; i < nmat; i += blockDim.x) {
-			const double2 v = __ldg(msrc + i);
-			mats[i] = make_float2((float)v.x, (float)v.y);
+		if (pre) {
+			for (int mi = 0; 64 * mi < nmat; ++mi)
+				tm_write_b(mats_b + (size_t)kTmBFloats * mi, msrc + 64 * mi, (int)tid,
+					   (int)blockDim.x);
+			/* read by the tensor cores (async proxy) */
+			asm volatile("fence.proxy.async.shared::cta;" ::);
+		} else {
+			for (int i = tid; i < nmat; i += blockDim.x) {
+				const double2 v = __ldg(msrc + i);
+				mats[i] = make_float2((float)v.x, (float)v.y);
+			}
 		}
 		for (int i = tid; i < 16; i += blockDim.x)
 			sq[i] = h->qpos[i];
 	}
 	if (tid == 0) {
-		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
 		asm volatile("fence.mbarrier_init.release.cluster;" ::);
 	}
 	if (warp == 0) {
@@ -975,13 +1015,13 @@ __global__ void __launch_bounds__(256, 2)
 	auto off_t = [&](int hh) -> uint64_t { return hh ? (off_t0 | (1ull << sq[8])) : off_t0; };
 	auto stid = [&](int hh) -> uint32_t { return hh ? (stid0 ^ s256) : stid0; };
 	/* passes: this thread's columns, one per row block it owns */
-	const uint32_t rb0 = 2u * (warp >> 2);
+	const uint32_t rb0 = 2u * wg;
 	uint32_t col[2];
 	col[0] = 128u * rb0 + 32u * (warp & 3u) + lane;
 	col[1] = col[0] + 128u;
 	const uint32_t ta = tbase + ((32u * (warp & 3u)) << 16); /* this warp's lane quarter */
-	const uint32_t mb = smem_u32(&mbar);
-	const uint32_t sb_hi = smem_u32(&sB[0][0]), sb_lo = smem_u32(&sB[1][0]);
+	const uint32_t mb = smem_u32(&mbar[wg]);
+	const bool issuer = tid == 128u * wg;
 	__syncthreads();
 	const uint64_t ntiles = h->ntiles;
 	const int ndep = (h->n - m + 3) >> 2;
@@ -1030,7 +1070,7 @@ __global__ void __launch_bounds__(256, 2)
 	};
 
 	double insq = 0.0, outsq = 0.0;
-	uint32_t phase = 0;
+	uint32_t phase = 0; /* of this warpgroup's mbarrier */
 	bool fault = false;
 	uint64_t t = next_tile(blockIdx.x);
 	if (t < ntiles)
@@ -1073,16 +1113,16 @@ __global__ void __launch_bounds__(256, 2)
 					if (((base & c.gc) != c.gc) || (base & c.ga))
 						continue; /* the same for every thread */
 				}
-				const float2 *mt = mats + 64 * (size_t)tc_matrix(d, scond, base);
-				{ /* B = R, entry (n, k), split into hi and lo */
-					const int n = (int)(tid >> 4), k = (int)(tid & 15u);
-					const float2 e = mt[8 * (n & 7) + (k & 7)];
-					const float v = ((n < 8) == (k < 8)) ? e.x : (n < 8 ? -e.y : e.y);
-					uint32_t hi, lo;
-					tf32_split(v, hi, lo);
-					const int o = umma_b_off(n, k);
-					sB[0][o] = __uint_as_float(hi);
-					sB[1][o] = __uint_as_float(lo);
+				const uint32_t mi = tc_matrix(d, scond, base);
+				uint32_t bsm;
+				if (pre) {
+					bsm = smem_u32(mats_b + (size_t)kTmBFloats * mi);
+				} else {
+					/* B' of this entry; the previous entry's MMAs were
+					 * waited for before the barrier that ended it */
+					tm_write_b(sB, mats + 64 * (size_t)mi, (int)tid, (int)blockDim.x);
+					asm volatile("fence.proxy.async.shared::cta;" ::);
+					bsm = smem_u32(sB);
 				}
 #pragma unroll
 				for (int j = 0; j < 2; ++j) {
@@ -1100,24 +1140,28 @@ __global__ void __launch_bounds__(256, 2)
 					tm_st16(ta + 64u + 16u * rb, vl);
 				}
 				asm volatile("tcgen05.wait::st.sync.aligned;" ::);
-				asm volatile("fence.proxy.async.shared::cta;" ::);
 				asm volatile("tcgen05.fence::before_thread_sync;" ::);
-				__syncthreads();
-				if (tid == 0 && !DK_TM_STARVED()) {
+				/* this warpgroup's rows are in tensor memory (and, per
+				 * entry, B' in shared memory: then the whole CTA) */
+				if (!pre)
+					__syncthreads();
+				else if (wg == 0)
+					asm volatile("bar.sync 1, 128;" ::: "memory");
+				else
+					asm volatile("bar.sync 2, 128;" ::: "memory");
+				if (issuer && !DK_TM_STARVED()) {
 					asm volatile("tcgen05.fence::after_thread_sync;" ::);
-					const uint64_t bh0 = umma_desc_k(sb_hi), bh1 = umma_desc_k(sb_hi + 512u);
-					const uint64_t bl0 = umma_desc_k(sb_lo), bl1 = umma_desc_k(sb_lo + 512u);
+					const uint64_t b0 = umma_desc_k(bsm), b1 = umma_desc_k(bsm + 1024u);
 #pragma unroll
-					for (uint32_t rb = 0; rb < 4; ++rb) {
-						const uint32_t dcol = tbase + 128u + 16u * rb;
+					for (uint32_t rb = rb0; rb < rb0 + 2u; ++rb) {
+						const uint32_t dcol = tbase + 128u + 32u * rb;
 						const uint32_t ah = tbase + 16u * rb, al = tbase + 64u + 16u * rb;
-						/* small terms first */
-						umma_tf32_ts(dcol, al, bh0, 0u);
-						umma_tf32_ts(dcol, al + 8u, bh1, 1u);
-						umma_tf32_ts(dcol, ah, bl0, 1u);
-						umma_tf32_ts(dcol, ah + 8u, bl1, 1u);
-						umma_tf32_ts(dcol, ah, bh0, 1u);
-						umma_tf32_ts(dcol, ah + 8u, bh1, 1u);
+						/* hi*hi -> D[0, 16), hi*lo -> D[16, 32) */
+						umma_tf32_ts(dcol, ah, b0, kTmIdesc32, 0u);
+						umma_tf32_ts(dcol, ah + 8u, b1, kTmIdesc32, 1u);
+						/* lo*hi -> D[16, 32) (B' rows 0..15 = R_hi) */
+						umma_tf32_ts(dcol + 16u, al, b0, kTmIdesc16, 1u);
+						umma_tf32_ts(dcol + 16u, al + 8u, b1, kTmIdesc16, 1u);
 					}
 					asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
 						     ::"r"(mb));
@@ -1126,14 +1170,15 @@ __global__ void __launch_bounds__(256, 2)
 				phase ^= 1u;
 				asm volatile("tcgen05.fence::after_thread_sync;" ::);
 				const bool ctl = (d.x & 0xffffu) == DK_GC_DENSE3 + 1;
-				/* both loads while the warp is converged (.sync.aligned),
-				 * before any per-column branch */
-				uint32_t y[2][16];
-				tm_ld16(ta + 128u + 16u * rb0, y[0]);
-				tm_ld16(ta + 128u + 16u * (rb0 + 1u), y[1]);
-				asm volatile("tcgen05.wait::ld.sync.aligned;" ::);
 #pragma unroll
 				for (int j = 0; j < 2; ++j) {
+					/* both loads while the warp is converged
+					 * (.sync.aligned), before any per-column branch */
+					uint32_t yh[16], yc[16];
+					const uint32_t dcol = ta + 128u + 32u * (rb0 + (uint32_t)j);
+					tm_ld16(dcol, yh);
+					tm_ld16(dcol + 16u, yc);
+					asm volatile("tcgen05.wait::ld.sync.aligned;" ::);
 					if (!ok)
 						continue;
 					if (ctl) { /* rare: controls off the pass bits */
@@ -1146,11 +1191,13 @@ __global__ void __launch_bounds__(256, 2)
 						const uint32_t so = cs[j] ^ ((r & 1) ? s0 : 0u) ^
 								    ((r & 2) ? s1 : 0u) ^ ((r & 4) ? s2 : 0u);
 						if (DK_IN_BOUNDS(so, tn_amp, CHK_SCATTER))
-							tile[so] = make_float2(__uint_as_float(y[j][r]),
-									       __uint_as_float(y[j][8 + r]));
+							tile[so] = make_float2(
+								__uint_as_float(yh[r]) + __uint_as_float(yc[r]),
+								__uint_as_float(yh[8 + r]) +
+									__uint_as_float(yc[8 + r]));
 					}
 				}
-				/* the scatters precede the next gather and the B rewrite;
+				/* the scatters precede the next gather and B' rewrite;
 				 * a timeout anywhere stops every thread */
 				asm volatile("tcgen05.fence::before_thread_sync;" ::);
 				if (__syncthreads_or(!ok)) {
@@ -1178,10 +1225,12 @@ __global__ void __launch_bounds__(256, 2)
 	}
 	cp_async_wait_all();
 	if (fault) {
-		/* the MMAs of the expired wait may still run: give them another
-		 * bounded wait before the tensor memory is released */
-		if (tid == 0) {
-			atomicAdd(&g_dk_tm_fault, 1u);
+		/* the MMAs of an expired wait may still run: give each
+		 * warpgroup's another bounded wait before the tensor memory is
+		 * released */
+		if (issuer) {
+			if (tid == 0)
+				atomicAdd(&g_dk_tm_fault, 1u);
 			(void)tm_wait(mb, phase ^ 1u);
 		}
 		insq = outsq = __longlong_as_double(0x7ff8000000000000ll);
@@ -2264,17 +2313,26 @@ static cudaError_t run_sweep_tc(const void *in, void *out, const unsigned char *
  * SM holds more than two CTAs of it (or of any kernel with the same floor)
  * and their 2 x 256 tensor-memory columns always fit in the SM's 512. */
 constexpr size_t kTmSmemFloor = 80u << 10;
-/* and at most this much, so that two of them fit on an SM */
-constexpr size_t kTmSmemMax = 104u << 10;
+/* and at most this much, so that two of them (with the kernel's static
+ * shared memory) fit on an SM */
+constexpr size_t kTmSmemMax = 106u << 10;
 
 static cudaError_t run_sweep_tm(const void *in, void *out, const unsigned char *dprog,
 				const dk_sweep_hdr *hp, int num_sms, const Scratch &s,
 				cudaStream_t st, int *blocks_out)
 {
-	size_t smem = 2 * (sizeof(float2) << 12) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
-		      (size_t)hp->ncond * sizeof(dk_gate_cond) +
-		      (size_t)hp->npass * sizeof(dk_pass_desc) +
-		      sizeof(float2) * ((hp->bytes - hp->mat_off) / 16);
+	const size_t nmat = (hp->bytes - hp->mat_off) / 16; /* complex entries */
+	const size_t mats_at = (2 * (sizeof(float2) << 12) + (size_t)hp->ngate * sizeof(dk_gate_desc) +
+				(size_t)hp->ncond * sizeof(dk_gate_cond) +
+				(size_t)hp->npass * sizeof(dk_pass_desc) + 1023) &
+			       ~(size_t)1023;
+	/* every matrix split once per CTA when they fit, else per entry */
+	int pre = 1;
+	size_t smem = mats_at + (nmat / 64) * kTmBFloats * sizeof(float);
+	if (smem > kTmSmemMax) {
+		pre = 0;
+		smem = mats_at + sizeof(float2) * nmat;
+	}
 	if (smem > kTmSmemMax)
 		return cudaErrorNotSupported; /* the caller runs the sweep on mma.sync */
 	if (smem < kTmSmemFloor)
@@ -2305,7 +2363,7 @@ static cudaError_t run_sweep_tm(const void *in, void *out, const unsigned char *
 		blocks = cap;
 	blocks = skip_balanced_grid(blocks, in, out, hp);
 	kern<<<(int)blocks, 256, smem, st>>>((const float2 *)in, (float2 *)out, dprog,
-					     s.partials);
+					     s.partials, pre);
 	*blocks_out = (int)blocks;
 	g_tm_ran.store(1);
 	return cudaGetLastError();

@@ -2207,7 +2207,9 @@ int g_num_sms = 148;
 
 std::atomic<unsigned long long> g_launches{0};
 int g_c64_tmem = 1;
+int g_tm_allow_presplit = 1;
 std::atomic<int> g_tm_ran{0};
+std::atomic<unsigned long long> g_tm_presplit{0}, g_tm_entry_b{0};
 
 /* ---------------------------------------------------------------------- */
 
@@ -2327,9 +2329,9 @@ static cudaError_t run_sweep_tm(const void *in, void *out, const unsigned char *
 				(size_t)hp->npass * sizeof(dk_pass_desc) + 1023) &
 			       ~(size_t)1023;
 	/* every matrix split once per CTA when they fit, else per entry */
-	int pre = 1;
+	int pre = g_tm_allow_presplit;
 	size_t smem = mats_at + (nmat / 64) * kTmBFloats * sizeof(float);
-	if (smem > kTmSmemMax) {
+	if (!pre || smem > kTmSmemMax) {
 		pre = 0;
 		smem = mats_at + sizeof(float2) * nmat;
 	}
@@ -2366,6 +2368,7 @@ static cudaError_t run_sweep_tm(const void *in, void *out, const unsigned char *
 					     s.partials, pre);
 	*blocks_out = (int)blocks;
 	g_tm_ran.store(1);
+	(pre ? g_tm_presplit : g_tm_entry_b).fetch_add(1, std::memory_order_relaxed);
 	return cudaGetLastError();
 }
 

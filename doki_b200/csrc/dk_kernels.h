@@ -20,6 +20,11 @@ extern std::atomic<unsigned long long> g_launches;
 extern int g_c64_tmem;
 /* set once a tcgen05 sweep has been launched (tm_fault_check has work) */
 extern std::atomic<int> g_tm_ran;
+/* tcgen05 sweeps may split all of a sweep's B operands once per CTA (1,
+ * default) or must split them per entry (0) */
+extern int g_tm_allow_presplit;
+/* tcgen05 sweeps launched with B split once per CTA / per entry */
+extern std::atomic<unsigned long long> g_tm_presplit, g_tm_entry_b;
 
 /* Faults counted by tcgen05 sweeps whose bounded waits expired since the
  * last call (0 = none); reads and clears the device counter on `st`. */

@@ -556,6 +556,9 @@ int dk_init(int device)
 	const char *tm = getenv("DK_C64_TMEM");
 	if (tm)
 		dk::g_c64_tmem = atoi(tm) ? 1 : 0;
+	const char *tp = getenv("DK_C64_TMEM_PRESPLIT");
+	if (tp)
+		dk::g_tm_allow_presplit = atoi(tp) ? 1 : 0;
 	g.inited = 1;
 	return DK_OK;
 }
@@ -1623,6 +1626,15 @@ int dk_get_mma_stats(uint64_t *entry_amplitudes)
 {
 	if (entry_amplitudes)
 		*entry_amplitudes = g.mma_entry_amps;
+	return DK_OK;
+}
+
+int dk_get_tm_stats(uint64_t *presplit, uint64_t *per_entry)
+{
+	if (presplit)
+		*presplit = dk::g_tm_presplit.load(std::memory_order_relaxed);
+	if (per_entry)
+		*per_entry = dk::g_tm_entry_b.load(std::memory_order_relaxed);
 	return DK_OK;
 }
 

@@ -1426,15 +1426,17 @@ static PyObject *doki_engine_set_fusion(PyObject *self, PyObject *args)
 
 static PyObject *doki_engine_stats(PyObject *self, PyObject *args)
 {
-	uint64_t l = 0, s = 0, g = 0, hi = 0, ho = 0, me = 0;
+	uint64_t l = 0, s = 0, g = 0, hi = 0, ho = 0, me = 0, tp = 0, te = 0;
 	dk_get_stats(&l, &s, &g);
 	dk_get_io_stats(&hi, &ho);
 	dk_get_mma_stats(&me);
-	return Py_BuildValue("{s:K,s:K,s:K,s:K,s:K,s:K}", "kernel_launches",
+	dk_get_tm_stats(&tp, &te);
+	return Py_BuildValue("{s:K,s:K,s:K,s:K,s:K,s:K,s:K,s:K}", "kernel_launches",
 			     (unsigned long long)l, "sweeps", (unsigned long long)s, "gates",
 			     (unsigned long long)g, "h2d_bytes", (unsigned long long)hi,
 			     "d2h_bytes", (unsigned long long)ho, "mma_entry_amplitudes",
-			     (unsigned long long)me);
+			     (unsigned long long)me, "tm_sweeps_presplit", (unsigned long long)tp,
+			     "tm_sweeps_entry_b", (unsigned long long)te);
 }
 
 static PyObject *doki_registry_compare(PyObject *self, PyObject *args)
@@ -2384,7 +2386,8 @@ static PyMethodDef DokiMethods[] = {
 	{ "engine_set_fusion", doki_engine_set_fusion, METH_VARARGS,
 	  "Enable (default) or disable multi-gate sweep fusion" },
 	{ "engine_stats", doki_engine_stats, METH_VARARGS,
-	  "Kernel launches, sweeps, gates and host<->device bytes so far" },
+	  "Kernel launches, sweeps, gates, host<->device bytes, tensor-core work and "
+	  "tcgen05 sweep counts so far" },
 	{ "registry_compare", doki_registry_compare, METH_VARARGS,
 	  "(fidelity, max amplitude error) between two registries of equal size" },
 	{ "engine_new_slot", doki_engine_new_slot, METH_VARARGS,

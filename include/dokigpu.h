@@ -197,6 +197,10 @@ int dk_get_stats(uint64_t *kernel_launches, uint64_t *sweeps,
  * products of 2 m8n8k4 k-steps per 64 amplitudes) or 96 TF32 MMA FMA
  * (complex64: 6 m16n8k8 MMAs per 64 amplitudes). */
 int dk_get_mma_stats(uint64_t *entry_amplitudes);
+/* complex64 sweeps launched on tcgen05 since load: with every B operand of
+ * the sweep split once per CTA into shared memory, and with B split per
+ * entry (sweeps whose matrices do not fit, or DK_C64_TMEM_PRESPLIT=0). */
+int dk_get_tm_stats(uint64_t *presplit, uint64_t *per_entry);
 /* Bytes copied host->device and device->host by this library since dk_init. */
 int dk_get_io_stats(uint64_t *h2d_bytes, uint64_t *d2h_bytes);
 /* Execute the gates queued on `s` now (normally deferred to the next read). */

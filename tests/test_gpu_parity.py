@@ -508,6 +508,50 @@ def test_complex64_brickwork_vs_complex128_oracle(dk_gpu, orc):
     assert np.allclose(d.registry_probs(a), orc.registry_probs(b), atol=ATOL_C64)
 
 
+_C64_RUN = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import doki_b200
+from doki_b200 import workloads as W
+d = doki_b200.load()
+n = int(sys.argv[2])
+c = W.scale_circuit(seed=3, n=n, depth=10, keep=6)
+a = W.run_ops(d, d.registry_new(n, False, 1), c.ops)
+np.save(sys.argv[3], np.asarray(d.registry_get_all(a, False)))
+st = d.engine_stats()
+print("tm", st["tm_sweeps_presplit"], st["tm_sweeps_entry_b"])
+"""
+
+
+@pytest.mark.parametrize("n", [14, 20])
+def test_complex64_tcgen05_b_split_per_entry_and_per_cta(dk_gpu, orc, n, tmp_path):
+    """Both ways the tcgen05 sweep gets its B operands -- split once per CTA
+    for the whole sweep (default) and split per entry (the path of sweeps
+    whose matrices do not fit, forced here by DK_C64_TMEM_PRESPLIT=0) --
+    against the complex128 oracle, each in its own process."""
+    import os
+    import subprocess
+    import sys
+    from tests.conftest import ROOT
+    c = W.scale_circuit(seed=3, n=n, depth=10, keep=6)
+    want = orc.registry_get_all(W.run_ops(orc, orc.registry_new(n), c.ops))
+    for pre in ("1", "0"):
+        out = str(tmp_path / f"amps{pre}.npy")
+        r = subprocess.run([sys.executable, "-c", _C64_RUN, ROOT, str(n), out],
+                           env=dict(os.environ, DK_C64_TMEM="1", DK_C64_TMEM_PRESPLIT=pre),
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-3000:]
+        tm = [ln for ln in r.stdout.splitlines() if ln.startswith("tm ")][0].split()
+        presplit, per_entry = int(tm[1]), int(tm[2])
+        if pre == "1":
+            assert presplit > 0, tm
+        else:
+            assert presplit == 0 and per_entry > 0, tm
+        got = np.load(out)
+        assert np.max(np.abs(got - want)) < ATOL_C64
+
+
 # ------------------------------------------------------- error behaviour ----
 
 def test_device_side_errors(dk_gpu):

@@ -59,6 +59,8 @@ def parse():
                         "served sample is scaled from their times by qubit count")
     p.add_argument("--serve-only", action="store_true",
                    help="run only the serving form and print its JSON object")
+    p.add_argument("--form-only", choices=("batch", "serve", "precision"),
+                   help="run only this form and print its JSON object")
     p.add_argument("--precision", choices=("c128", "c64"), default="c128",
                    help="register precision of the plain workload (c64: split-TF32 "
                         "tensor products, FP64 norms)")
@@ -459,12 +461,26 @@ def batch_form(d, torch):
                      "rho_bytes": int(rho.nbytes), "tile_bits": tune["tile_bits"],
                      "fold": tune["fold"], "ctas_per_sm": tune["ctas_per_sm"],
                      "autotune_cached": tune["cached"],
+                     "autotune_objective": "host planning + one device run",
                      "autotune_trials": [{k: t[k] for k in ("fold", "tile_bits", "ctas_per_sm")}
-                                         | {"ms": t["seconds"] * 1e3}
+                                         | {"ms": t["seconds"] * 1e3,
+                                            "plan_ms": t["plan_s"] * 1e3}
                                          for t in tune["trials"]]}
     fid, err = engines["c64"].compare(engines["c128"])
+    # the same figures on the host for a sample of the registers (every
+    # 64th), from downloaded states: an independent check of the device
+    # comparison
+    hf, he = [], []
+    for c in range(0, fb.count, 64):
+        x, y = engines["c64"].state(c), engines["c128"].state(c)
+        hf.append(abs(np.vdot(x, y)) ** 2 / (np.vdot(x, x).real * np.vdot(y, y).real))
+        he.append(float(np.max(np.abs(x / np.linalg.norm(x) - y / np.linalg.norm(y)))))
     res["c64"].update({"min_fidelity": float(fid.min()), "max_amp_err": float(err.max()),
-                       "fidelity_vs": "the complex128 batch of the same 4096 circuits"})
+                       "fidelity_vs": "the complex128 batch of the same 4096 circuits",
+                       "host_check": {"registers": len(hf), "min_fidelity": float(min(hf)),
+                                      "max_amp_err": float(max(he)),
+                                      "device_min_fidelity_same_registers":
+                                          float(fid[::64].min())}})
     for eng in engines.values():
         eng.close()
     plain = plain_circuits_per_s(d, fb)
@@ -724,14 +740,20 @@ def reference_arm(args, rank, world):
     }), flush=True)
 
 
-def serve_only(args):
-    """The serving form alone (for runs over the whole request stream)."""
+def form_only(args, name):
+    """One form alone (e.g. the serving form over the whole request
+    stream)."""
+    import torch
+
     import doki_b200
     d = doki_b200.load()
+    fn = {"batch": lambda: batch_form(d, torch),
+          "serve": lambda: serve_form(d, args.serve_requests, args.serve_plain),
+          "precision": lambda: precision_form(d)}[name]
     t0 = time.perf_counter()
-    out = serve_form(d, args.serve_requests, args.serve_plain)
+    out = fn()
     out["wall_s"] = time.perf_counter() - t0
-    print(json.dumps({"form": "serve", **out}), flush=True)
+    print(json.dumps({"form": name, **out}), flush=True)
 
 
 def main():
@@ -739,8 +761,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.serve_only:
-        serve_only(args)
+    if args.serve_only or args.form_only:
+        form_only(args, "serve" if args.serve_only else args.form_only)
         return
     if args.impl == "reference":
         reference_arm(args, rank, world)

@@ -191,8 +191,10 @@ def autotune(batch: FlatBatch, precision: int, tile_bits: Iterable[int] = (10, 1
     """Pick the dense-block fusion of the plan (`fold`: -1 every gate on its
     own, 0 the planner's default, larger values fold runs of gates into 8x8
     products more readily), tile bits (streamed registers) and CTAs per SM
-    by timing the batch under every combination; results, with every trial,
-    are cached per (device, precision, batch signature)."""
+    by timing the batch under every combination.  A batch is planned once
+    and run once, so the objective is the host planning and upload time of
+    the combination plus one device run; results, with every trial, are
+    cached per (device, precision, batch signature)."""
     path = cache_path or default_cache_path()
     key = f"{device_name}|{_signature(batch, precision)}"
     try:
@@ -200,20 +202,25 @@ def autotune(batch: FlatBatch, precision: int, tile_bits: Iterable[int] = (10, 1
             cache = json.load(f)
     except (OSError, ValueError):
         cache = {}
-    if key in cache and "fold" in cache[key]:
+    if key in cache and cache[key].get("objective") == "plan+run":
         return dict(cache[key], cached=True)
     trials = []
     for fold in folds:
         for tb in tile_bits:
+            t0 = time.perf_counter()
             eng = BatchEngine(batch, precision, tile_bits=tb, fold=fold)
+            plan_s = time.perf_counter() - t0
             for c in ctas:
                 eng.set_ctas(c)
+                run_s = time_runs(eng, reps)
                 trials.append({"fold": fold, "tile_bits": tb, "ctas_per_sm": c,
-                               "seconds": time_runs(eng, reps)})
+                               "plan_s": plan_s, "seconds": run_s,
+                               "objective_s": plan_s + run_s})
             eng.close()
-    best = min(trials, key=lambda t: t["seconds"])
+    best = min(trials, key=lambda t: t["objective_s"])
     result = {"fold": best["fold"], "tile_bits": best["tile_bits"],
-              "ctas_per_sm": best["ctas_per_sm"], "seconds": best["seconds"], "trials": trials}
+              "ctas_per_sm": best["ctas_per_sm"], "seconds": best["seconds"],
+              "plan_s": best["plan_s"], "objective": "plan+run", "trials": trials}
     cache[key] = result
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)

@@ -92,6 +92,10 @@ def test_autotuner_caches(dk_gpu, small_batch, tmp_path):
     assert r1["tile_bits"] in (10, 12) and not r1["cached"]
     r2 = autotune(small_batch, 1, tile_bits=(10, 12), ctas=(1,), reps=1, cache_path=cache)
     assert r2["cached"] and r2["tile_bits"] == r1["tile_bits"]
+    # the pick minimises host planning plus one device run, over every trial
+    assert r1["objective"] == "plan+run"
+    best = min(t["plan_s"] + t["seconds"] for t in r1["trials"])
+    assert r1["plan_s"] + r1["seconds"] == best
 
 
 def test_batch_config_depths_vs_oracle(dk_gpu, orc, oracle_mod):

@@ -198,24 +198,61 @@ def finish_job(d, reg, n, keep, mask, rolls):
     return probs, res, mat
 
 
-def tensor_roofline(entry_amps, sweep_s, c64, clk, steps):
+def library_gemm_tflops(torch, c64, n=8192, reps=5):
+    """Throughput of the library GEMM of the sweep's arithmetic, timed here
+    with CUDA events: cuBLAS DGEMM (complex128 sweeps) or cuBLAS TF32 SGEMM
+    (complex64), n x n x n, after one warm-up."""
+    dt = torch.float32 if c64 else torch.float64
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = bool(c64)
+    try:
+        a = torch.randn(n, n, device="cuda", dtype=dt)
+        b = torch.randn(n, n, device="cuda", dtype=dt)
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return 2.0 * n ** 3 * reps / (ms / 1e3) / 1e12
+
+
+def tensor_roofline(entry_amps, sweep_s, c64, clk, steps, lib_tflops=None, tcgen05=False):
     """Tensor-pipe work of the timed sweeps.  One matrix entry applied to one
     amplitude is 24 FP64 MMA FMA (complex128: three real m8n8k4 products of
-    two k-steps per 64 amplitudes) or 96 TF32 MMA FMA (complex64: six m16n8k8
-    MMAs per 64 amplitudes).  The FP64 peak is the MMA op rate ncu reports
+    two k-steps per 64 amplitudes) or 96 TF32 MMA FMA (complex64: three
+    TF32 products per 8x16 by 16x16 real block).  The peak is the measured
+    library GEMM of the same arithmetic (cuBLAS DGEMM / TF32 SGEMM on this
+    GPU) when given; for FP64 the MMA op rate ncu reports
     (sm__ops_path_tensor_src_fp64: 128 per SM per cycle) x SMs x the median SM
-    clock of the run; no TF32 figure is measured, so complex64 has none."""
+    clock of the run is given beside it."""
     import torch
     fma = entry_amps * (96 if c64 else 24)
     achieved = 2.0 * fma / max(sweep_s, 1e-12) / 1e12
-    out = {"pipe": "tf32 mma.sync m16n8k8" if c64 else "fp64 mma.sync m8n8k4",
-           "achieved": achieved, "unit": "TFLOP/s", "flops_per_step": 2.0 * fma / steps}
+    pipe = ("tf32 tcgen05.mma (M=128, N=32/16)" if tcgen05 else "tf32 mma.sync m16n8k8") \
+        if c64 else "fp64 mma.sync m8n8k4"
+    out = {"pipe": pipe, "achieved": achieved, "unit": "TFLOP/s",
+           "flops_per_step": 2.0 * fma / steps}
+    if lib_tflops:
+        out.update({"peak": lib_tflops, "frac": achieved / lib_tflops,
+                    "peak_kind": "measured cuBLAS " + ("TF32 SGEMM" if c64 else "DGEMM")
+                                 + " 8192^3 on this GPU"})
     if not c64:
         mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-        peak = 128.0 * sms * mhz * 1e6 / 1e12
-        out.update({"peak": peak, "frac": achieved / peak,
-                    "peak_kind": f"ncu FP64 MMA op rate 128/SM/cycle x {sms} SMs x {mhz:g} MHz"})
+        nominal = 128.0 * sms * mhz * 1e6 / 1e12
+        out.update({"peak_op_rate": nominal, "frac_op_rate": achieved / nominal,
+                    "peak_op_rate_kind": f"ncu FP64 MMA op rate 128/SM/cycle x {sms} SMs x "
+                                         f"{mhz:g} MHz"})
+        if not lib_tflops:
+            out.update({"peak": nominal, "frac": achieved / nominal,
+                        "peak_kind": out["peak_op_rate_kind"]})
     return out
 
 
@@ -347,6 +384,8 @@ def engine_arm(args, rank, world, local_rank):
     value = job_rate(world, layers, dev_ms / 1e3)
     e2e_value = job_rate(world, layers, e2e_s)
     c64 = args.precision == "c64"
+    tcgen05 = c64 and os.environ.get("DK_C64_TMEM", "1") != "0"
+    lib_tflops = library_gemm_tflops(torch, c64) if rank == 0 and world == 1 else None
     state_bytes = (8 if c64 else 16) << n
     avg_sweep_s = (sweep_ms / 1e3) / max(1, nsweeps)
     achieved = 2 * state_bytes / avg_sweep_s / 1e9
@@ -363,7 +402,9 @@ def engine_arm(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f32" if c64 else "f64", "data": "synthetic",
         "config": workload_config(n, depth, c, args.precision),
         "roofline": {"bound": "hbm",
-                     "kernel": ("k_sweep_tc<float> (fused gate sweep, split-TF32 tensor-core "
+                     "kernel": ("k_sweep_tm (fused gate sweep, split-TF32 tcgen05 products "
+                                "in tensor memory)" if tcgen05 else
+                                "k_sweep_tc<float> (fused gate sweep, split-TF32 tensor-core "
                                 "passes)" if c64 else
                                 "k_sweep_tc<double> (fused gate sweep, FP64 tensor-core passes)"),
                      "achieved": achieved, "peak": peak,
@@ -378,7 +419,8 @@ def engine_arm(args, rank, world, local_rank):
                 "d2h_bytes_per_step": (io1["d2h_bytes"] - io0["d2h_bytes"]) // args.steps},
         "tensor_roofline": tensor_roofline(st1["mma_entry_amplitudes"] -
                                            st0["mma_entry_amplitudes"],
-                                           sweep_ms / 1e3, c64, clk, args.steps),
+                                           sweep_ms / 1e3, c64, clk, args.steps,
+                                           lib_tflops, tcgen05),
         "gpu_launches": st1["kernel_launches"] - st0["kernel_launches"],
         "clocks": clk,
         "fusion": not args.no_fusion,

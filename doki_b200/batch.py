@@ -127,8 +127,15 @@ class BatchEngine:
                     "dk_batch_rho")
         return out
 
-    def rho_all(self) -> Tuple[np.ndarray, np.ndarray]:
-        out = np.empty(self.rho_elems, dtype=np.complex128)
+    def rho_all(self, out: Optional[np.ndarray] = None) -> Tuple[np.ndarray, np.ndarray]:
+        """Every register's reduced density matrix, concatenated, and their
+        offsets.  `out` (complex128, at least rho_elems long; e.g. a view of
+        a reused page-locked buffer) receives them when given."""
+        if out is None:
+            out = np.empty(self.rho_elems, dtype=np.complex128)
+        elif out.dtype != np.complex128 or out.size < self.rho_elems or \
+                not out.flags.c_contiguous:
+            raise BatchError("rho_all: out must be contiguous complex128 of rho_elems")
         offs = np.empty(self.batch.count, dtype=np.uint64)
         self._check(lib().dk_batch_rho_all(self._h, _ptr(out.view(np.float64), _dp),
                                            _ptr(offs, _u64p)), "dk_batch_rho_all")

@@ -61,6 +61,12 @@ def test_batch_graph_relaunch_is_deterministic(dk_gpu, small_batch):
     eng.sync()
     again, _ = eng.rho_all()
     assert np.array_equal(first, again)
+    # into a caller's (larger, page-locked) buffer
+    import torch
+    buf = torch.empty(2 * eng.rho_elems + 8, dtype=torch.float64,
+                      pin_memory=True).numpy().view(np.complex128)
+    into, _ = eng.rho_all(out=buf)
+    assert np.array_equal(into[:eng.rho_elems], first)
     eng.close()
 
 

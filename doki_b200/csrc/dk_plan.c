@@ -222,14 +222,17 @@ static void pass_tables(dk_pass_desc *pd, const uint8_t *pb, int m, int sw)
  * (half-warp) accesses conflict free. */
 static int phase_score(const uint32_t *pmask, int cnt, uint32_t W, int m, int res)
 {
+	/* a pass scores when its lane bits L meet every residue class mod res */
+	uint32_t cls[8] = { 0 };
+	for (int b = 0; b < m; b++)
+		cls[b % res] |= 1u << b;
 	int score = 0;
 	for (int i = 0; i < cnt; i++) {
 		const uint32_t L = ((1u << m) - 1u) & ~pmask[i] & ~W;
-		uint32_t seen = 0;
-		for (int b = 0; b < m; b++)
-			if (L & (1u << b))
-				seen |= 1u << (b % res);
-		score += popc(seen) == res;
+		int all = 1;
+		for (int r = 0; r < res && all; r++)
+			all = (L & cls[r]) != 0;
+		score += all;
 	}
 	return score;
 }
@@ -949,13 +952,11 @@ static int foldable(const dk_flat_op *op, const int8_t *loc_of, const uint32_t *
 		if (lb < 0 || preg[lb] == 0xffffffffu)
 			return 0;
 	}
-	const uint64_t c = op->cm | op->am;
-	for (unsigned q = 0; q < 64; q++)
-		if (c & (UINT64_C(1) << q)) {
-			const int lb = loc_of[q];
-			if (lb < 0 || preg[lb] == 0xffffffffu)
-				return 0;
-		}
+	for (uint64_t c = op->cm | op->am; c; c &= c - 1) {
+		const int lb = loc_of[__builtin_ctzll(c)];
+		if (lb < 0 || preg[lb] == 0xffffffffu)
+			return 0;
+	}
 	return 1;
 }
 

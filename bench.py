@@ -505,7 +505,7 @@ def batch_form(d, torch):
                      "plan_and_upload_s": build_s,
                      "e2e_circuits_per_s": fb.count / (build_s + out_s),
                      "e2e_parts_s": {"plan_and_upload": build_s,
-                                     "run_and_copy_rho": out_s},
+                                     "run_and_copy_rho": out_s, **eng.build_times()},
                      "rho_host_buffer": "page-locked, allocated once and reused",
                      "rho_bytes": int(rho.nbytes), "tile_bits": tune["tile_bits"],
                      "fold": tune["fold"], "ctas_per_sm": tune["ctas_per_sm"],

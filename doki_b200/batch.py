@@ -50,6 +50,7 @@ def lib() -> ctypes.CDLL:
         L.dk_batch_rho_elems.restype = ctypes.c_uint64
         L.dk_batch_state.argtypes = [ctypes.c_void_p, ctypes.c_uint, _dp]
         L.dk_batch_compare.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _dp, _dp]
+        L.dk_batch_build_times.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         L.dk_batch_error.argtypes = [ctypes.c_void_p]
         L.dk_batch_error.restype = ctypes.c_char_p
         L.dk_batch_free.argtypes = [ctypes.c_void_p]
@@ -105,6 +106,14 @@ class BatchEngine:
             L = lib()
             raise BatchError(f"{what}: {L.dk_strerror(rc).decode()} "
                              f"({L.dk_batch_error(self._h).decode()})")
+
+    def build_times(self) -> Dict[str, float]:
+        """Host seconds of the build: planning, blob assembly, device
+        allocation and upload."""
+        v = [ctypes.c_double(), ctypes.c_double(), ctypes.c_double()]
+        self._check(lib().dk_batch_build_times(self._h, *[ctypes.byref(x) for x in v]),
+                    "dk_batch_build_times")
+        return {"plan_s": v[0].value, "assemble_s": v[1].value, "upload_s": v[2].value}
 
     def set_ctas(self, ctas_per_sm: int):
         self._check(lib().dk_batch_set_ctas(self._h, ctas_per_sm), "dk_batch_set_ctas")

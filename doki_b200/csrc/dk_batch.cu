@@ -21,6 +21,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -317,6 +318,9 @@ struct dk_batch {
 	std::vector<cudaEvent_t> ev;
 	cudaGraphExec_t graph = nullptr;
 	int graph_keep_states = -1;
+	/* host seconds of dk_batch_build: planning (all threads), assembling
+	 * the program blob and register tables, device allocation and upload */
+	double t_plan = 0.0, t_assemble = 0.0, t_upload = 0.0;
 	char err[128] = { 0 };
 };
 
@@ -470,6 +474,8 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 			dk_plan_free(&plan);
 		}
 	};
+	typedef std::chrono::steady_clock clk;
+	const auto t0 = clk::now();
 	unsigned T = std::thread::hardware_concurrency();
 	if (T == 0)
 		T = 1;
@@ -484,6 +490,13 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 		plan_some(0, T);
 		for (auto &th : pool)
 			th.join();
+	}
+	const auto t1 = clk::now();
+	{
+		size_t total = 0;
+		for (unsigned c = 0; c < num_circuits; ++c)
+			total += planned[c].prog.size() + 16;
+		blob.reserve(total);
 	}
 	for (unsigned c = 0; c < num_circuits; ++c) {
 		if (planned[c].rc) {
@@ -521,6 +534,7 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 	for (auto &cl : b->classes)
 		std::stable_sort(cl.regs.begin(), cl.regs.end(),
 				 [](const dk_breg &x, const dk_breg &y) { return x.n > y.n; });
+	const auto t2 = clk::now();
 	cudaError_t e = cudaMalloc(&b->dblob, blob.size() ? blob.size() : 16);
 	if (e == cudaSuccess)
 		e = cudaMemcpy(b->dblob, blob.data(), blob.size(), cudaMemcpyHostToDevice);
@@ -562,6 +576,10 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 		delete b;
 		return r2;
 	}
+	const auto t3 = clk::now();
+	b->t_plan = std::chrono::duration<double>(t1 - t0).count();
+	b->t_assemble = std::chrono::duration<double>(t2 - t1).count();
+	b->t_upload = std::chrono::duration<double>(t3 - t2).count();
 	*out = b;
 	return DK_OK;
 }
@@ -795,6 +813,20 @@ int dk_batch_compare(dk_batch *x, dk_batch *y, double *fidelity, double *max_amp
 }
 
 const char *dk_batch_error(const dk_batch *b) { return b ? b->err : ""; }
+
+int dk_batch_build_times(const dk_batch *b, double *plan_s, double *assemble_s,
+			 double *upload_s)
+{
+	if (!b)
+		return DK_ERR_ARG;
+	if (plan_s)
+		*plan_s = b->t_plan;
+	if (assemble_s)
+		*assemble_s = b->t_assemble;
+	if (upload_s)
+		*upload_s = b->t_upload;
+	return DK_OK;
+}
 
 void dk_batch_free(dk_batch *b)
 {

@@ -267,6 +267,11 @@ int dk_batch_state(dk_batch *b, unsigned circuit, double *out);
  * (fidelity, max_amp_err: one double per circuit). */
 int dk_batch_compare(dk_batch *x, dk_batch *y, double *fidelity, double *max_amp_err);
 const char *dk_batch_error(const dk_batch *b);
+/* Host seconds dk_batch_build spent planning the circuits (on all host
+ * threads), assembling the program blob and register tables, and allocating
+ * and uploading the device buffers. */
+int dk_batch_build_times(const dk_batch *b, double *plan_s, double *assemble_s,
+			 double *upload_s);
 void dk_batch_free(dk_batch *b);
 
 /* ---- allocation-free marginals (no counterpart in the reference) --------

@@ -67,6 +67,9 @@ def test_batch_graph_relaunch_is_deterministic(dk_gpu, small_batch):
                       pin_memory=True).numpy().view(np.complex128)
     into, _ = eng.rho_all(out=buf)
     assert np.array_equal(into[:eng.rho_elems], first)
+    bt = eng.build_times()
+    assert set(bt) == {"plan_s", "assemble_s", "upload_s"}
+    assert bt["plan_s"] > 0 and min(bt.values()) >= 0
     eng.close()
 
 

@@ -1887,6 +1887,18 @@ __global__ void __launch_bounds__(256)
 	}
 }
 
+/* The gather above when the kept qubits are the low k ones: X is the
+ * register itself, widened to FP64 -- two amplitudes per 16-byte load. */
+__global__ void __launch_bounds__(256)
+	k_widen_c64(const float4 *__restrict__ d, double4 *M, uint64_t pairs)
+{
+	for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < pairs;
+	     e += (uint64_t)gridDim.x * blockDim.x) {
+		const float4 v = __ldcs(d + e);
+		M[e] = make_double4((double)v.x, (double)v.y, (double)v.z, (double)v.w);
+	}
+}
+
 __global__ void __launch_bounds__(256)
 	k_herm_fill(const double2 *__restrict__ C, double2 *rho, uint64_t dim)
 {
@@ -2821,6 +2833,13 @@ cudaError_t launch_gather_kept(int prec, const void *d, unsigned n,
 	const uint64_t trace = full & ~keep_mask;
 	const int k = __builtin_popcountll(keep_mask);
 	const uint64_t total = 1ull << n;
+	if (prec == DK_C64 && keep_mask == (1ull << k) - 1ull && n >= 1) {
+		const uint64_t pairs = total >> 1;
+		k_widen_c64<<<grid_for(pairs, 256 * 4, g_num_sms * 8), 256, 0, st>>>(
+			(const float4 *)d, (double4 *)M, pairs);
+		g_launches += 1;
+		return cudaGetLastError();
+	}
 	const int blocks = grid_for(total, 256 * 4, g_num_sms * 8);
 	if (prec == DK_C128)
 		k_gather_kept<double><<<blocks, 256, 0, st>>>((const double2 *)d,

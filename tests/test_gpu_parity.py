@@ -396,7 +396,7 @@ def test_density_algebra_vs_oracle(dk_gpu, orc, oracle_mod):
 
 
 @pytest.mark.parametrize("n,keep_bits,prec", [(12, 3, 2), (16, 5, 2), (16, 6, 2), (18, 8, 2),
-                                               (20, 10, 2), (18, 7, 1), (17, 9, 2)])
+                                               (20, 10, 2), (18, 7, 1), (20, 10, 1), (17, 9, 2)])
 def test_reduced_density_sizes(dk_gpu, orc, oracle_mod, n, keep_bits, prec):
     """The tensor-core product X X^H over kept sets from 8 to 1024 amplitudes:
     one or many output tiles, split and unsplit traced ranges, contiguous and

@@ -22,6 +22,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <memory>
+#include <new>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -396,7 +398,8 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 		cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev);
 	}
 	const size_t amp = precision == DK_C128 ? 16 : 8;
-	std::vector<unsigned char> blob;
+	std::unique_ptr<unsigned char[]> blob; /* programs, uninitialised between them */
+	size_t blob_len = 0;
 	std::vector<int> class_of_m(13, -1);
 	b->rho_off.resize(num_circuits);
 	b->state_off.resize(num_circuits);
@@ -492,28 +495,48 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 			th.join();
 	}
 	const auto t1 = clk::now();
-	{
-		size_t total = 0;
-		for (unsigned c = 0; c < num_circuits; ++c)
-			total += planned[c].prog.size() + 16;
-		blob.reserve(total);
-	}
-	for (unsigned c = 0; c < num_circuits; ++c) {
+	for (unsigned c = 0; c < num_circuits; ++c)
 		if (planned[c].rc) {
 			rc = planned[c].rc;
 			delete b;
 			return rc;
 		}
+	/* each circuit's programs at a 16-byte aligned offset of one blob,
+	 * copied in by all host threads */
+	std::vector<size_t> at(num_circuits);
+	for (unsigned c = 0; c < num_circuits; ++c) {
+		const size_t pad = ((blob_len + 15) & ~(size_t)15) - blob_len;
+		at[c] = blob_len + pad;
+		blob_len = at[c] + planned[c].prog.size();
+	}
+	blob.reset(new (std::nothrow) unsigned char[blob_len ? blob_len : 16]);
+	if (!blob) {
+		delete b;
+		return DK_ERR_ALLOC;
+	}
+	{
+		auto copy_some = [&](unsigned first, unsigned stride) {
+			for (unsigned c = first; c < num_circuits; c += stride) {
+				if (!planned[c].prog.empty())
+					memcpy(blob.get() + at[c], planned[c].prog.data(),
+					       planned[c].prog.size());
+				std::vector<unsigned char>().swap(planned[c].prog);
+			}
+		};
+		std::vector<std::thread> pool;
+		for (unsigned t = 1; t < T; ++t)
+			pool.emplace_back(copy_some, t, T);
+		copy_some(0, T);
+		for (auto &th : pool)
+			th.join();
+	}
+	for (unsigned c = 0; c < num_circuits; ++c) {
 		const unsigned n = num_qubits[c];
 		const unsigned keep = keep_qubits[c];
 		const int m = n <= 12 ? (int)n : tile_bits;
 		dk_breg reg;
 		memset(&reg, 0, sizeof(reg));
-		const size_t start = (blob.size() + 15) & ~(size_t)15;
-		blob.resize(start);
-		reg.prog = start;
-		blob.insert(blob.end(), planned[c].prog.begin(), planned[c].prog.end());
-		std::vector<unsigned char>().swap(planned[c].prog);
+		reg.prog = at[c];
 		reg.nsweep = planned[c].nsweep;
 		reg.n = n;
 		reg.keep = keep;
@@ -535,10 +558,10 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 		std::stable_sort(cl.regs.begin(), cl.regs.end(),
 				 [](const dk_breg &x, const dk_breg &y) { return x.n > y.n; });
 	const auto t2 = clk::now();
-	cudaError_t e = cudaMalloc(&b->dblob, blob.size() ? blob.size() : 16);
-	if (e == cudaSuccess)
-		e = cudaMemcpy(b->dblob, blob.data(), blob.size(), cudaMemcpyHostToDevice);
-	b->blob_bytes = blob.size();
+	cudaError_t e = cudaMalloc(&b->dblob, blob_len ? blob_len : 16);
+	if (e == cudaSuccess && blob_len)
+		e = cudaMemcpy(b->dblob, blob.get(), blob_len, cudaMemcpyHostToDevice);
+	b->blob_bytes = blob_len;
 	if (e == cudaSuccess)
 		e = cudaMalloc(&b->dstates, amp * b->state_amps);
 	if (e == cudaSuccess)

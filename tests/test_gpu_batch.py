@@ -103,8 +103,11 @@ def test_autotuner_caches(dk_gpu, small_batch, tmp_path):
     assert r2["cached"] and r2["tile_bits"] == r1["tile_bits"]
     # the pick minimises host planning plus one device run, over every trial
     assert r1["objective"] == "plan+run"
-    best = min(t["plan_s"] + t["seconds"] for t in r1["trials"])
+    best = min(t["objective_s"] for t in r1["trials"])
     assert r1["plan_s"] + r1["seconds"] == best
+    for t in r1["trials"]:
+        same_fold = [u["plan_s"] for u in r1["trials"] if u["fold"] == t["fold"]]
+        assert t["objective_s"] == min(same_fold) + t["seconds"]
 
 
 def test_batch_config_depths_vs_oracle(dk_gpu, orc, oracle_mod):

@@ -326,6 +326,27 @@ struct dk_batch {
 	char err[128] = { 0 };
 };
 
+/* fn(t, T) for t = 0 .. T-1, on T threads (the caller's included); shares
+ * whose thread cannot be started run on the caller, so no exception leaves
+ * this C-ABI library */
+template <typename F> static void run_strided(unsigned T, F &fn)
+{
+	std::vector<std::thread> pool;
+	std::vector<unsigned> inline_shares;
+	for (unsigned t = 1; t < T; ++t) {
+		try {
+			pool.emplace_back(fn, t, T);
+		} catch (...) {
+			inline_shares.push_back(t);
+		}
+	}
+	fn(0u, T);
+	for (unsigned t : inline_shares)
+		fn(t, T);
+	for (auto &th : pool)
+		th.join();
+}
+
 static int batch_cuda_fail(dk_batch *b, cudaError_t e)
 {
 	if (b)
@@ -364,13 +385,12 @@ static void batch_release_device(dk_batch *b)
 
 extern "C" {
 
-int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qubits,
-		   const unsigned *keep_qubits, const uint64_t *op_start, const unsigned *op_k,
-		   const unsigned *op_targets, const uint64_t *op_controls,
-		   const uint64_t *op_anticontrols, const uint64_t *op_matrix,
-		   const double *matrices, int tile_bits, int fold, dk_batch **out)
+static int batch_build(int precision, unsigned num_circuits, const unsigned *num_qubits,
+		       const unsigned *keep_qubits, const uint64_t *op_start, const unsigned *op_k,
+		       const unsigned *op_targets, const uint64_t *op_controls,
+		       const uint64_t *op_anticontrols, const uint64_t *op_matrix,
+		       const double *matrices, int tile_bits, int fold, dk_batch **out)
 {
-	DK_TRACE();
 	if (!out || (precision != DK_C64 && precision != DK_C128) || !num_qubits ||
 	    !keep_qubits || !op_start || (num_circuits == 0))
 		return DK_ERR_ARG;
@@ -422,8 +442,13 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 			Planned &pl = planned[c];
 			const unsigned n = num_qubits[c];
 			const uint64_t o0 = op_start[c], o1 = op_start[c + 1];
-			gates.resize(o1 - o0);
-			flat.resize(o1 - o0);
+			try {
+				gates.resize(o1 - o0);
+				flat.resize(o1 - o0);
+			} catch (...) {
+				pl.rc = DK_ERR_ALLOC;
+				continue;
+			}
 			for (uint64_t i = o0; i < o1; ++i) {
 				dk_gate &gt = gates[i - o0];
 				gt.refcount = 1;
@@ -460,7 +485,12 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 				const dk_sweep_hdr *h =
 					(const dk_sweep_hdr *)(plan.blob + plan.steps[st].prog_off);
 				const size_t at = pl.prog.size();
-				pl.prog.resize(at + h->bytes);
+				try {
+					pl.prog.resize(at + h->bytes);
+				} catch (...) {
+					pl.rc = DK_ERR_ALLOC;
+					break;
+				}
 				memcpy(pl.prog.data() + at, h, h->bytes);
 				if (precision == DK_C64) {
 					/* store the matrices in the amplitude precision, in place */
@@ -487,12 +517,7 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 	if (T > num_circuits)
 		T = num_circuits;
 	{
-		std::vector<std::thread> pool;
-		for (unsigned t = 1; t < T; ++t)
-			pool.emplace_back(plan_some, t, T);
-		plan_some(0, T);
-		for (auto &th : pool)
-			th.join();
+		run_strided(T, plan_some);
 	}
 	const auto t1 = clk::now();
 	for (unsigned c = 0; c < num_circuits; ++c)
@@ -523,12 +548,7 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 				std::vector<unsigned char>().swap(planned[c].prog);
 			}
 		};
-		std::vector<std::thread> pool;
-		for (unsigned t = 1; t < T; ++t)
-			pool.emplace_back(copy_some, t, T);
-		copy_some(0, T);
-		for (auto &th : pool)
-			th.join();
+		run_strided(T, copy_some);
 	}
 	for (unsigned c = 0; c < num_circuits; ++c) {
 		const unsigned n = num_qubits[c];
@@ -605,6 +625,23 @@ int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qub
 	b->t_upload = std::chrono::duration<double>(t3 - t2).count();
 	*out = b;
 	return DK_OK;
+}
+
+int dk_batch_build(int precision, unsigned num_circuits, const unsigned *num_qubits,
+		   const unsigned *keep_qubits, const uint64_t *op_start, const unsigned *op_k,
+		   const unsigned *op_targets, const uint64_t *op_controls,
+		   const uint64_t *op_anticontrols, const uint64_t *op_matrix,
+		   const double *matrices, int tile_bits, int fold, dk_batch **out)
+{
+	DK_TRACE();
+	/* host allocation failures (std::bad_alloc) become a status code */
+	try {
+		return batch_build(precision, num_circuits, num_qubits, keep_qubits, op_start, op_k,
+				   op_targets, op_controls, op_anticontrols, op_matrix, matrices,
+				   tile_bits, fold, out);
+	} catch (...) {
+		return DK_ERR_ALLOC;
+	}
 }
 
 int dk_batch_set_ctas(dk_batch *b, int ctas_per_sm)

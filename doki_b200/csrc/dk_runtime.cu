@@ -19,6 +19,7 @@
 
 #include <atomic>
 #include <mutex>
+#include <new>
 #include <vector>
 
 #include "dk_internal.h"
@@ -93,7 +94,9 @@ struct SlotLock {
 
 int create_slot(int id)
 {
-	Slot *sl = new Slot();
+	Slot *sl = new (std::nothrow) Slot();
+	if (!sl)
+		return DK_ERR_ALLOC;
 	cudaError_t e = cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking);
 	if (e == cudaSuccess)
 		e = cudaMalloc(&sl->scratch.partials,
@@ -247,10 +250,24 @@ int check_live(dk_state *s)
 }
 
 /* Execute the pending gates of `s` (see the file comment). */
+static int flush_queued(dk_state *s);
+
+/* Run the register's queued gates; host allocation failures (std::bad_alloc
+ * from the plan's buffers) become DK_ERR_ALLOC, so no exception leaves the
+ * C ABI. */
 int flush(dk_state *s)
 {
 	if (!s->pending)
 		return DK_OK;
+	try {
+		return flush_queued(s);
+	} catch (...) {
+		return DK_ERR_ALLOC;
+	}
+}
+
+static int flush_queued(dk_state *s)
+{
 	DK_TRACE();
 	const unsigned n = s->n;
 	const int prec = s->prec;

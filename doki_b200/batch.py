@@ -17,7 +17,7 @@ import ctypes
 import json
 import os
 import time
-from typing import Dict, Iterable, Optional, Tuple
+from typing import Dict, Iterable, List, Optional, Tuple
 
 import numpy as np
 
@@ -201,6 +201,22 @@ def default_cache_path() -> str:
                                        "autotune.json"))
 
 
+def pick_trial(trials: List[Dict]) -> Tuple[Dict, float]:
+    """The autotuner's choice among timed trials ({fold, tile_bits,
+    ctas_per_sm, plan_s, seconds}): planning work depends on the fold, not
+    on the tile width or CTAs per SM, so each trial is charged its fold's
+    fastest measured planning (timing noise in planning cannot pick a slower
+    kernel configuration) plus its device run; sets each trial's
+    `objective_s` and returns the best trial and its fold's planning time."""
+    fold_plan: Dict[int, float] = {}
+    for t in trials:
+        fold_plan[t["fold"]] = min(fold_plan.get(t["fold"], t["plan_s"]), t["plan_s"])
+    for t in trials:
+        t["objective_s"] = fold_plan[t["fold"]] + t["seconds"]
+    best = min(trials, key=lambda t: t["objective_s"])
+    return best, fold_plan[best["fold"]]
+
+
 def autotune(batch: FlatBatch, precision: int, tile_bits: Iterable[int] = (10, 11, 12),
              ctas: Iterable[int] = (1, 2), folds: Iterable[int] = (-1, 0, 400), reps: int = 2,
              cache_path: Optional[str] = None, device_name: str = "") -> Dict:
@@ -230,22 +246,12 @@ def autotune(batch: FlatBatch, precision: int, tile_bits: Iterable[int] = (10, 1
                 eng.set_ctas(c)
                 run_s = time_runs(eng, reps)
                 trials.append({"fold": fold, "tile_bits": tb, "ctas_per_sm": c,
-                               "plan_s": plan_s, "seconds": run_s,
-                               "objective_s": plan_s + run_s})
+                               "plan_s": plan_s, "seconds": run_s})
             eng.close()
-    # planning work depends on the fold, not on the tile width or CTAs per SM:
-    # charge each trial its fold's fastest measured planning, so that timing
-    # noise in planning cannot pick a slower kernel configuration
-    fold_plan = {}
-    for t in trials:
-        fold_plan[t["fold"]] = min(fold_plan.get(t["fold"], t["plan_s"]), t["plan_s"])
-    for t in trials:
-        t["objective_s"] = fold_plan[t["fold"]] + t["seconds"]
-    best = min(trials, key=lambda t: t["objective_s"])
+    best, plan = pick_trial(trials)
     result = {"fold": best["fold"], "tile_bits": best["tile_bits"],
               "ctas_per_sm": best["ctas_per_sm"], "seconds": best["seconds"],
-              "plan_s": fold_plan[best["fold"]], "objective": "plan+run",
-              "trials": trials}
+              "plan_s": plan, "objective": "plan+run", "trials": trials}
     cache[key] = result
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)

@@ -22,10 +22,11 @@ module: one request at a time, one ``registry_apply`` call per gate.
 """
 from __future__ import annotations
 
+import collections
 import threading
 import time
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional, Sequence
+from typing import Deque, Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -155,15 +156,26 @@ def run_plain(d, reqs: Sequence[Request], precision: int = 2,
 
 
 class Server:
-    """Continuous batching over `workers` engine slots under an HBM budget."""
+    """Continuous batching over `workers` engine slots under an HBM budget.
+
+    Requests are admitted in arrival order as slots and memory free up.
+    With `express` > 0, that many of the slots take only requests of at most
+    `express_max_qubits` qubits, and such a small request may be admitted
+    ahead of an earlier larger one that is waiting for a slot or memory
+    (larger requests keep their order among themselves), so small requests
+    do not queue behind the large ones that occupy the device."""
 
     def __init__(self, d, workers: int = 8, budget_bytes: float = 150e9, precision: int = 1,
-                 deadline_s: float = 600.0):
+                 deadline_s: float = 600.0, express: int = 0, express_max_qubits: int = 20):
+        if not 0 <= express < workers:
+            raise ValueError("express slots must leave at least one general slot")
         self.d = d
         self.workers = workers
         self.budget = budget_bytes
         self.precision = precision
         self.deadline_s = deadline_s
+        self.express = express
+        self.express_max_qubits = express_max_qubits
         self.slots = [0] + [d.engine_new_slot() for _ in range(workers - 1)]
 
     def run(self, reqs: Sequence[Request], keep_results: bool = False) -> Dict:
@@ -218,21 +230,56 @@ class Server:
             if time.perf_counter() - t0 > self.deadline_s:
                 raise TimeoutError(f"serving run exceeded {self.deadline_s} s")
 
+        express = set(range(self.workers - self.express, self.workers))
+        # arrived, not yet admitted: the general class and (with express
+        # slots) the small class, each in arrival order
+        waiting_general: Deque[Request] = collections.deque()
+        waiting_small: Deque[Request] = collections.deque()
+
+        def place(req: Request, slots: List[int]) -> bool:
+            need = 2 * req.state_bytes(self.precision)
+            if not slots or (state["mem"] + need > self.budget and state["mem"] > 0):
+                return False
+            w = slots[0]
+            state["free"].remove(w)
+            state["mem"] += need
+            queues[w].append(req)
+            lock.notify_all()
+            return True
+
+        def admit() -> None:
+            while waiting_general and place(
+                    waiting_general[0], [w for w in state["free"] if w not in express]):
+                waiting_general.popleft()
+            # small requests: express slots, and general ones nobody waits for
+            while waiting_small:
+                slots = [w for w in state["free"] if w in express]
+                if not waiting_general:
+                    slots += [w for w in state["free"] if w not in express]
+                if not place(waiting_small[0], slots):
+                    break
+                waiting_small.popleft()
+
         try:
-            for req in reqs:
-                wait = req.arrival - (time.perf_counter() - t0)
-                if wait > 0:
-                    time.sleep(wait)
-                need = 2 * req.state_bytes(self.precision)
+            i = 0
+            while i < len(reqs) or waiting_general or waiting_small:
+                while i < len(reqs) and reqs[i].arrival <= time.perf_counter() - t0:
+                    req = reqs[i]
+                    small = bool(express) and req.n <= self.express_max_qubits
+                    (waiting_small if small else waiting_general).append(req)
+                    i += 1
                 with lock:
-                    while not state["free"] or (state["mem"] + need > self.budget
-                                                and state["mem"] > 0):
-                        lock.wait(timeout=1.0)
+                    admit()
+                    if waiting_general or waiting_small:
+                        # wait for a completion, or for the next arrival
+                        to_next = (reqs[i].arrival - (time.perf_counter() - t0)
+                                   if i < len(reqs) else 1.0)
+                        lock.wait(timeout=min(1.0, max(1e-4, to_next)))
                         check()
-                    w = state["free"].pop(0)
-                    state["mem"] += need
-                    queues[w].append(req)
-                    lock.notify_all()
+                if not (waiting_general or waiting_small) and i < len(reqs):
+                    wait = reqs[i].arrival - (time.perf_counter() - t0)
+                    if wait > 0:
+                        time.sleep(wait)
             with lock:
                 while state["done"] < len(reqs):
                     lock.wait(timeout=1.0)

@@ -112,3 +112,41 @@ def test_plain_path_runs_one_request_at_a_time_gate_by_gate():
     assert out["requests"] == 5 and len(out["seconds"]) == 5
     assert d.max_live == 1
     assert len(calls) == sum(r.flat().count for r in reqs)
+
+
+class SizedDelay(FakeDoki):
+    """Requests of more than 20 qubits take long on the fake device."""
+
+    def _finish(self, reg):
+        time.sleep(0.3 if reg["n"] > 20 else 0.002)
+        with self.lock:
+            self.live -= 1
+            self.mem -= (8 if reg["precision"] == 1 else 16) << reg["n"]
+
+
+def mixed_stream():
+    # two large requests first, then small ones arriving right behind them
+    reqs = []
+    for i, n in enumerate([24, 24] + [10] * 12):
+        reqs.append(S.Request(rid=i, arrival=0.001 * i, n=n, depth=1, seed=i,
+                              terminal="probs"))
+    return reqs
+
+
+def test_express_slots_let_small_requests_pass_large_ones():
+    """With 2 slots both held by large requests, small requests queue behind
+    them (plain arrival order); with one express slot they run meanwhile,
+    while the large ones keep their order on the general slot."""
+    plain = S.Server(SizedDelay(), workers=2, budget_bytes=1e12, precision=1)
+    out = plain.run(mixed_stream(), keep_results=False)
+    fast = S.Server(SizedDelay(), workers=2, budget_bytes=1e12, precision=1, express=1)
+    out2 = fast.run(mixed_stream(), keep_results=False)
+    assert out["requests"] == out2["requests"] == 14
+    # the small requests' median latency: behind the large ones vs not
+    assert out["p50_ms"] > 250
+    assert out2["p50_ms"] < 100
+
+
+def test_express_slots_leave_a_general_slot():
+    with pytest.raises(ValueError):
+        S.Server(FakeDoki(), workers=2, express=2)
